@@ -1,0 +1,330 @@
+// apr.cu -- CP-APR (multiplicative update) on the device.
+//
+// Replaces cp_apr_alto (IntelLabs/ALTO include/apr.hpp:984-1376) and
+// tt_logLikelihood<LIT> (:851-982).  Order of operations follows the
+// reference: KruskalModelNormalize, then per outer iteration and mode n the
+// kappa fix (iter > 0), RedistributeLambda, up to max_inner rounds of
+// {Phi, KKT violation, B *= Phi} with the early exit when the violation is
+// below epsilon (skipped in bench mode), and KruskalModelNormalizeMode.  The
+// KKT violation and the log-likelihood accumulate in FP64.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dense.cuh"
+#include "mttkrp_plan.h"
+
+namespace altob {
+
+altob_status check_model(const altob_tensor* t, altob_dtype ft, void* const* dU, u64 rank);
+
+// |min(B, 1 - Phi)| max-reduced (apr.hpp:1210-1216); with `mult`, also
+// B *= Phi (apr.hpp:1226-1231) in the same pass.
+template <typename FT>
+__global__ void k_kkt(FT* __restrict__ B, const FT* __restrict__ Phi, u64 n, double* __restrict__ kkt, int mult)
+{
+    double m = 0.0;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x) {
+        const double b = (double)B[e], p = (double)Phi[e];
+        m = fmax(m, fabs(fmin(b, 1.0 - p)));
+        if (mult) B[e] = (FT)(b * p);
+    }
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(reinterpret_cast<unsigned long long*>(kkt), (unsigned long long)__double_as_longlong(m));
+}
+
+template <typename FT>
+__global__ void k_mult(FT* __restrict__ B, const FT* __restrict__ Phi, u64 n)
+{
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x)
+        B[e] = (FT)((double)B[e] * (double)Phi[e]);
+}
+
+// Kappa fix (apr.hpp:1176-1189).
+template <typename FT>
+__global__ void k_kappa(FT* __restrict__ B, const FT* __restrict__ Phi, u64 n, double kappa_tol, double kappa)
+{
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x)
+        if ((double)B[e] < kappa_tol && (double)Phi[e] > 1.0) B[e] = (FT)((double)B[e] + kappa);
+}
+
+template <typename FT>
+struct LLArgs {
+    const u64* klo;
+    const u64* khi;
+    const void* vals;
+    u64 nnz;
+    int nmode, R;
+    double eps;
+    const FT* U[ALTOB_MAX_MODES];
+    Decoder dec;
+};
+
+// sum_nnz v * log(max(sum_r prod_n U_n[i_n, r], eps)) (apr.hpp:913-943).
+template <typename FT, typename VT, int KW>
+__global__ void __launch_bounds__(256) k_loglik(LLArgs<FT> a, double* __restrict__ acc)
+{
+    const VT* vals = reinterpret_cast<const VT*>(a.vals);
+    double s = 0.0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.nnz; i += (u64)gridDim.x * blockDim.x) {
+        u32 w[4];
+        split_key(a.klo[i], KW == 2 ? a.khi[i] : 0ull, w);
+        const FT* rows[ALTOB_MAX_MODES];
+        for (int m = 0; m < a.nmode; ++m)
+            rows[m] = a.U[m] + (size_t)decode_mode(w, a.dec.md[m], a.dec.nwords) * a.R;
+        double tmp = 0.0;
+        for (int r = 0; r < a.R; ++r) {
+            double p = 1.0;
+            for (int m = 0; m < a.nmode; ++m) p *= (double)__ldg(rows[m] + r);
+            tmp += p;
+        }
+        if (tmp < a.eps) tmp = a.eps;
+        s += (double)vals[i] * log(tmp);
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
+}
+
+static int ew_grid(u64 n)
+{
+    u64 b = (n + 256 * 8 - 1) / (256 * 8);
+    return (int)std::max<u64>(1, std::min<u64>(b, (u64)num_sms() * 8));
+}
+
+template <typename FT>
+static altob_status loglik_sum(const altob_tensor* t, FT** U, int R, double eps, double* acc, cudaStream_t st)
+{
+    ALTOB_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), st));
+    if (t->nnz == 0) return ALTOB_OK;
+    LLArgs<FT> a;
+    memset(&a, 0, sizeof(a));
+    a.klo = t->d_klo;
+    a.khi = t->d_khi;
+    a.vals = t->d_vals;
+    a.nnz = t->nnz;
+    a.nmode = t->nmode;
+    a.R = R;
+    a.eps = eps;
+    for (int m = 0; m < t->nmode; ++m) a.U[m] = U[m];
+    a.dec = t->dec;
+    const int g = ew_grid(t->nnz);
+#define LLK(VT)                                                                      \
+    do {                                                                             \
+        if (t->kw == 2) k_loglik<FT, VT, 2><<<g, 256, 0, st>>>(a, acc);              \
+        else k_loglik<FT, VT, 1><<<g, 256, 0, st>>>(a, acc);                         \
+    } while (0)
+    if (t->vdt == ALTOB_U32) LLK(u32);
+    else if (t->vdt == ALTOB_F64) LLK(double);
+    else LLK(float);
+#undef LLK
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+struct AprScratch {
+    double *lam, *colacc, *kkt, *G, *inner, *fit, *normAT, *ll, *fsum;
+    int* info;
+};
+
+// tt_logLikelihood (apr.hpp:851-982): lambda into mode 0, log-likelihood
+// minus sum(U_0), then mode 0 renormalised by its column 1-norms.
+template <typename FT>
+static altob_status loglik_impl(altob_tensor* t, FT** U, double* lam, double* colacc, double* ll, double* fsum,
+                                int R, double eps, double* out, cudaStream_t st)
+{
+    ALTOB_TRY(mul_cols<FT>(U[0], t->dims[0], R, lam, st));
+    ALTOB_TRY(vec_fill(lam, R, 1.0, st));
+    ALTOB_TRY(loglik_sum<FT>(t, U, R, eps, ll, st));
+    ALTOB_TRY(sum_all<FT>(U[0], t->dims[0] * (u64)R, fsum, st));
+    ALTOB_TRY(colsum_abs<FT>(U[0], t->dims[0], R, colacc, st));
+    ALTOB_TRY(div_cols<FT>(U[0], t->dims[0], R, colacc, st));
+    ALTOB_TRY(vec_mul(lam, colacc, R, st));
+    double h[2];
+    ALTOB_CUDA(cudaMemcpyAsync(&h[0], ll, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ALTOB_CUDA(cudaMemcpyAsync(&h[1], fsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ALTOB_CUDA(cudaStreamSynchronize(st));
+    *out = h[0] - h[1];
+    return ALTOB_OK;
+}
+
+template <typename FT>
+static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int max_iters, int max_inner,
+                                double eps, double eps_div_zero, double kappa_tol, double kappa, int dobench,
+                                double* summary, cudaStream_t st)
+{
+    const int N = t->nmode;
+    const altob_dtype ft = sizeof(FT) == 8 ? ALTOB_F64 : ALTOB_F32;
+    size_t phi_elems = 0;
+    std::vector<size_t> phi_off(N);
+    for (int n = 0; n < N; ++n) {
+        phi_off[n] = phi_elems;
+        phi_elems += (t->dims[n] * R + 63) & ~(size_t)63;
+    }
+    size_t nd = 4 * (size_t)R + (size_t)N * R * R + 16;
+    size_t bytes = nd * sizeof(double) + 256 + phi_elems * sizeof(FT) + 256;
+    void* base = nullptr;
+    ALTOB_TRY(tensor_scratch(t, bytes, &base));
+    double* d = (double*)base;
+    AprScratch s;
+    s.lam = d;
+    d += R;
+    s.colacc = d;
+    d += R;
+    s.inner = d;
+    d += R;
+    s.G = d;
+    d += (size_t)N * R * R;
+    s.kkt = d;
+    d += 8;  // one per mode
+    s.fit = d++;
+    s.normAT = d++;
+    s.ll = d++;
+    s.fsum = d++;
+    s.info = (int*)d;
+    d += 2;
+    FT* phi_base = (FT*)(((uintptr_t)d + 255) & ~(uintptr_t)255);
+    std::vector<FT*> Phi(N);
+    for (int n = 0; n < N; ++n) Phi[n] = phi_base + phi_off[n];
+
+    // KruskalModelNormalize (src/kruskal_model.cpp:128-176)
+    ALTOB_TRY(vec_from<FT>(s.lam, lam_io, R, st));
+    for (int n = 0; n < N; ++n) {
+        ALTOB_TRY(colsum_abs<FT>(U[n], t->dims[n], R, s.colacc, st));
+        ALTOB_TRY(div_cols<FT>(U[n], t->dims[n], R, s.colacc, st));
+        ALTOB_TRY(vec_mul(s.lam, s.colacc, R, st));
+    }
+    std::vector<double> kkt_iter(max_iters + 1, 0.0), kmode(N, 0.0);
+    std::vector<int> ninner(max_iters + 1, 0);
+    int iter;
+    for (iter = 0; iter < max_iters; ++iter) {
+        bool converged = false;
+        if (dobench) ALTOB_CUDA(cudaMemsetAsync(s.kkt, 0, N * sizeof(double), st));
+        for (int n = 0; n < N; ++n) {
+            const u64 sz = t->dims[n] * (u64)R;
+            FT* B = U[n];
+            if (iter > 0 && sz) {
+                k_kappa<FT><<<ew_grid(sz), 256, 0, st>>>(B, Phi[n], sz, kappa_tol, kappa);
+                ALTOB_LAUNCH_CHECK();
+            }
+            ALTOB_TRY(mul_cols<FT>(B, t->dims[n], R, s.lam, st));  // RedistributeLambda
+            ALTOB_TRY(vec_fill(s.lam, R, 1.0, st));
+            for (int inner = 0; inner < max_inner; ++inner) {
+                ninner[iter]++;
+                ALTOB_TRY(phi_device(t, n, ft, (void* const*)U, (u64)R, eps_div_zero, Phi[n], st));
+                if (dobench) {
+                    // no early exit: the violation of the last round is what the reference reports
+                    ALTOB_CUDA(cudaMemsetAsync(s.kkt + n, 0, sizeof(double), st));
+                    if (sz) k_kkt<FT><<<ew_grid(sz), 256, 0, st>>>(B, Phi[n], sz, s.kkt + n, 1);
+                    ALTOB_LAUNCH_CHECK();
+                } else {
+                    ALTOB_CUDA(cudaMemsetAsync(s.kkt + n, 0, sizeof(double), st));
+                    if (sz) k_kkt<FT><<<ew_grid(sz), 256, 0, st>>>(B, Phi[n], sz, s.kkt + n, 0);
+                    ALTOB_LAUNCH_CHECK();
+                    double kv = 0.0;
+                    ALTOB_CUDA(cudaMemcpyAsync(&kv, s.kkt + n, sizeof(double), cudaMemcpyDeviceToHost, st));
+                    ALTOB_CUDA(cudaStreamSynchronize(st));
+                    kmode[n] = kv;
+                    if (kv < eps) break;
+                    if (sz) k_mult<FT><<<ew_grid(sz), 256, 0, st>>>(B, Phi[n], sz);
+                    ALTOB_LAUNCH_CHECK();
+                }
+            }
+            // KruskalModelNormalizeMode (src/kruskal_model.cpp:178-222)
+            ALTOB_TRY(colsum_abs<FT>(B, t->dims[n], R, s.colacc, st));
+            ALTOB_TRY(div_cols<FT>(B, t->dims[n], R, s.colacc, st));
+            ALTOB_TRY(vec_mul(s.lam, s.colacc, R, st));
+        }
+        if (dobench) {
+            ALTOB_CUDA(cudaMemcpyAsync(kmode.data(), s.kkt, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+            ALTOB_CUDA(cudaStreamSynchronize(st));
+        }
+        kkt_iter[iter] = kmode[0];
+        for (int n = 1; n < N; ++n) kkt_iter[iter] = std::fmax(kkt_iter[iter], kmode[n]);
+        // apr.hpp:1261; the first iteration has no predecessor to compare with
+        if (iter > 0 && std::fabs(kkt_iter[iter] - kkt_iter[iter - 1]) <= eps * eps && !dobench) converged = true;
+        if (converged) break;
+    }
+    int tot_inner = 0;
+    for (int i = 0; i < iter; ++i) tot_inner += ninner[i];
+    double ll = 0.0;
+    ALTOB_TRY(loglik_impl<FT>(t, U, s.lam, s.colacc, s.ll, s.fsum, R, eps_div_zero, &ll, st));
+
+    // least-squares fit of the final model (apr.hpp:1301-1330)
+    for (int n = 0; n < N - 1; ++n)
+        ALTOB_TRY(gram<FT>(U[n], t->dims[n], R, s.G + (size_t)n * R * R, nullptr, nullptr, nullptr, nullptr, st));
+    FT* mt = Phi[N - 1];
+    {
+        std::vector<void*> tmpU(N);
+        for (int n = 0; n < N; ++n) tmpU[n] = U[n];
+        tmpU[N - 1] = mt;
+        ALTOB_TRY(mttkrp_device(t, N - 1, ft, tmpU.data(), (u64)R, 0, ALTOB_ALGO_AUTO, st));
+    }
+    ALTOB_TRY(gram<FT>(U[N - 1], t->dims[N - 1], R, s.G + (size_t)(N - 1) * R * R, nullptr, nullptr, mt, s.inner,
+                       st));
+    ALTOB_TRY(value_sumsq(t, s.normAT, st));
+    double normAT = 0.0;
+    ALTOB_CUDA(cudaMemcpyAsync(&normAT, s.normAT, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ALTOB_CUDA(cudaStreamSynchronize(st));
+    ALTOB_TRY(fit_from(s.G, N, R, s.lam, s.inner, normAT, s.fit, st));
+    double fit = 0.0;
+    ALTOB_CUDA(cudaMemcpyAsync(&fit, s.fit, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ALTOB_TRY(vec_to<FT>(lam_io, s.lam, R, st));
+    ALTOB_CUDA(cudaStreamSynchronize(st));
+    if (summary) {
+        summary[0] = ll;
+        summary[1] = fit;
+        summary[2] = iter > 0 ? kkt_iter[iter - 1] : kkt_iter[0];
+        summary[3] = iter;
+        summary[4] = tot_inner;
+    }
+    return ALTOB_OK;
+}
+
+}  // namespace altob
+
+using namespace altob;
+
+extern "C" {
+
+altob_status altob_cp_apr(altob_tensor* t, altob_dtype ftype, void* const* d_factors, void* d_lambda, uint64_t rank,
+                          int max_iters, int max_inner, double epsilon, double eps_div_zero, double kappa_tol,
+                          double kappa, int dobench, double* summary, void* stream)
+{
+    ALTOB_TRY(check_model(t, ftype, d_factors, rank));
+    if (!d_lambda) return fail(ALTOB_ERR_ARG, "lambda is NULL");
+    if (max_iters < 1 || max_inner < 1) return fail(ALTOB_ERR_ARG, "iteration counts must be >= 1");
+    if (t->nnz == 0) return fail(ALTOB_ERR_ARG, "CP-APR on an empty tensor");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ftype == ALTOB_F64)
+        return cp_apr_impl<double>(t, (double**)d_factors, (double*)d_lambda, (int)rank, max_iters, max_inner,
+                                   epsilon, eps_div_zero, kappa_tol, kappa, dobench, summary, st);
+    return cp_apr_impl<float>(t, (float**)d_factors, (float*)d_lambda, (int)rank, max_iters, max_inner, epsilon,
+                              eps_div_zero, kappa_tol, kappa, dobench, summary, st);
+}
+
+altob_status altob_loglik(altob_tensor* t, altob_dtype ftype, void* const* d_factors, void* d_lambda, uint64_t rank,
+                          double eps_div_zero, double* loglik, void* stream)
+{
+    ALTOB_TRY(check_model(t, ftype, d_factors, rank));
+    if (!d_lambda || !loglik) return fail(ALTOB_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int R = (int)rank;
+    void* base = nullptr;
+    ALTOB_TRY(tensor_scratch(t, (4 * (size_t)R + 8) * sizeof(double), &base));
+    double* d = (double*)base;
+    double *lam = d, *colacc = d + R, *ll = d + 2 * R, *fsum = d + 2 * R + 1;
+    if (ftype == ALTOB_F64) {
+        ALTOB_TRY(vec_from<double>(lam, (const double*)d_lambda, R, st));
+        ALTOB_TRY(loglik_impl<double>(t, (double**)d_factors, lam, colacc, ll, fsum, R, eps_div_zero, loglik, st));
+        ALTOB_TRY(vec_to<double>((double*)d_lambda, lam, R, st));
+    } else {
+        ALTOB_TRY(vec_from<float>(lam, (const float*)d_lambda, R, st));
+        ALTOB_TRY(loglik_impl<float>(t, (float**)d_factors, lam, colacc, ll, fsum, R, eps_div_zero, loglik, st));
+        ALTOB_TRY(vec_to<float>((float*)d_lambda, lam, R, st));
+    }
+    ALTOB_CUDA(cudaStreamSynchronize(st));
+    return ALTOB_OK;
+}
+
+}  // extern "C"

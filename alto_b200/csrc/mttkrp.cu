@@ -1,0 +1,262 @@
+// mttkrp.cu -- MTTKRP and Phi entry points.
+//
+// altob_mttkrp replaces mttkrp_alto_par (IntelLabs/ALTO include/alto.hpp:
+// 617-623) including its dispatch on fiber reuse (alto.hpp:554-563) and its
+// += semantics; altob_phi replaces CalculatePhi_alto_par (include/apr.hpp:
+// 297-303).
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+
+#include "mttkrp_launch.cuh"
+#include "mttkrp_plan.h"
+
+namespace altob {
+
+static int env_int(const char* name, int dflt)
+{
+    const char* v = getenv(name);
+    return v && *v ? atoi(v) : dflt;
+}
+
+static int next_pow2(int x)
+{
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+static int floor_pow2(long long x)
+{
+    int p = 1;
+    while ((long long)p * 2 <= x) p <<= 1;
+    return p;
+}
+
+bool ptr_aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, bool cache, TiledPlan* pl)
+{
+    const int V = (int)(16 / fsz);
+    pl->vec = (aligned && R % V == 0) ? V : 1;
+    pl->lpn = pl->vec == 1 ? 32 : std::max(2, std::min(32, next_pow2((int)((R + pl->vec - 1) / pl->vec))));
+    const u64 per_pass = (u64)pl->lpn * pl->vec;
+    if ((R + per_pass - 1) / per_pass > (u64)MT_CHMAX)
+        return fail(ALTOB_ERR_UNSUPPORTED, "rank too large for the MTTKRP kernel (max " +
+                                               std::to_string(MT_CHMAX * 32 * V) + ")");
+    pl->tile = env_int("ALTOB_TILE", 1024);
+    pl->tile = std::max(256, (pl->tile / 256) * 256);
+    int cache_bytes = env_int("ALTOB_CACHE_BYTES", 64 * 1024);
+    long long rows = (long long)cache_bytes / (long long)(R * fsz);
+    pl->hslots = (cache && rows >= 16) ? std::min(floor_pow2(rows), 4096) : 0;
+    pl->smem = tiled_smem(t->nmode, pl->tile, pl->hslots, (int)R, fsz);
+    return ALTOB_OK;
+}
+
+template <typename FT, typename VT>
+static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, void* dout, u64 R, bool phi,
+                                 double eps, const u32* perm, bool cache, cudaStream_t st)
+{
+    bool aligned = ptr_aligned16(dout);
+    for (int m = 0; m < t->nmode; ++m) aligned = aligned && ptr_aligned16(dU[m]);
+    TiledPlan pl;
+    ALTOB_TRY(plan_tiled(t, R, sizeof(FT), aligned, cache, &pl));
+    TiledArgs<FT> a;
+    memset(&a, 0, sizeof(a));
+    a.klo = t->d_klo;
+    a.khi = t->d_khi;
+    a.vals = t->d_vals;
+    a.perm = perm;
+    a.nnz = t->nnz;
+    a.ntiles = (t->nnz + pl.tile - 1) / pl.tile;
+    a.nmode = t->nmode;
+    a.target = mode;
+    a.R = (int)R;
+    a.tile = pl.tile;
+    a.hslots = pl.hslots;
+    a.eps = (FT)eps;
+    for (int m = 0; m < t->nmode; ++m) a.U[m] = (const FT*)dU[m];
+    a.out = (FT*)dout;
+    a.dec = t->dec;
+    TiledCfg c;
+    c.kw = t->kw;
+    c.lpn = pl.lpn;
+    c.vec = pl.vec;
+    c.phi = phi ? 1 : 0;
+    c.smem = pl.smem;
+    c.grid = dim3(0);
+    int bps = 0;
+    ALTOB_TRY((launch_tiled<FT, VT>(a, c, st, &bps)));
+    if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "MTTKRP kernel does not fit on an SM");
+    u64 cap = (u64)bps * num_sms();
+    c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, cap)));
+    return launch_tiled<FT, VT>(a, c, st, nullptr);
+}
+
+template <typename FT>
+static altob_status run_tiled(altob_tensor* t, int mode, void* const* dU, void* dout, u64 R, bool phi, double eps,
+                              const u32* perm, bool cache, cudaStream_t st)
+{
+    const bool f64 = sizeof(FT) == 8;
+    if (t->vdt == ALTOB_U32) return run_tiled_vt<FT, u32>(t, mode, dU, dout, R, phi, eps, perm, cache, st);
+    if ((t->vdt == ALTOB_F64) == f64) return run_tiled_vt<FT, FT>(t, mode, dU, dout, R, phi, eps, perm, cache, st);
+    return fail(ALTOB_ERR_UNSUPPORTED, "stored value dtype does not match the compute dtype");
+}
+
+template <typename FT>
+static altob_status run_atomic_cr(altob_tensor* t, int mode, void* const* dU, u64 R, cudaStream_t st)
+{
+    u128 crm = t->cr_masks[mode];
+    if (!crm) return fail(ALTOB_ERR_ARG, "ATOMIC_CR needs a CR bit for the target mode");
+    CrArgsK<FT> a;
+    memset(&a, 0, sizeof(a));
+    a.klo = t->d_klo;
+    a.khi = t->d_khi;
+    a.vals = t->d_vals;
+    a.nnz = t->nnz;
+    a.nprtn = t->nprtn;
+    a.per = (t->nnz + t->nprtn - 1) / t->nprtn;
+    a.nmode = t->nmode;
+    a.target = mode;
+    a.R = (int)R;
+    a.crword = (u64)crm ? 0 : 1;
+    a.crbit = (u64)crm ? (u64)crm : (u64)(crm >> 64);
+    if (a.crword == 1 && t->kw != 2) return fail(ALTOB_ERR_ARG, "CR bit outside the stored key");
+    for (int m = 0; m < t->nmode; ++m) a.U[m] = (const FT*)dU[m];
+    a.out = (FT*)dU[mode];
+    a.dec = t->dec;
+    const bool f64 = sizeof(FT) == 8;
+    if (t->vdt == ALTOB_U32) return launch_atomic_cr<FT, u32>(a, t->kw, st);
+    if ((t->vdt == ALTOB_F64) == f64) return launch_atomic_cr<FT, FT>(a, t->kw, st);
+    return fail(ALTOB_ERR_UNSUPPORTED, "stored value dtype does not match the compute dtype");
+}
+
+altob_algo resolve_algo(const altob_tensor* t, int mode, altob_algo algo)
+{
+    if (algo != ALTOB_ALGO_AUTO) return algo;
+    if (fib_reuse(t, mode) > 4) return ALTOB_ALGO_TILED;
+    if (t->is_oidx && t->d_oidx[mode]) return ALTOB_ALGO_OPSCHED;
+    if (t->cr_masks[mode]) return ALTOB_ALGO_ATOMIC_CR;
+    return ALTOB_ALGO_ATOMIC;
+}
+
+altob_status mttkrp_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, int accumulate,
+                           altob_algo algo, cudaStream_t st)
+{
+    if (!t || !dU) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    if (R < 1) return fail(ALTOB_ERR_ARG, "rank must be >= 1");
+    if (ft != ALTOB_F64 && ft != ALTOB_F32) return fail(ALTOB_ERR_ARG, "compute dtype must be F64 or F32");
+    for (int m = 0; m < t->nmode; ++m)
+        if (!dU[m]) return fail(ALTOB_ERR_ARG, "a factor pointer is NULL");
+    const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    if (!accumulate) ALTOB_CUDA(cudaMemsetAsync(dU[mode], 0, t->dims[mode] * R * fsz, st));
+    if (t->nnz == 0) return ALTOB_OK;
+    algo = resolve_algo(t, mode, algo);
+    const u32* perm = nullptr;
+    bool cache = true;
+    switch (algo) {
+    case ALTOB_ALGO_TILED: break;
+    case ALTOB_ALGO_ATOMIC: cache = false; break;
+    case ALTOB_ALGO_OPSCHED:
+        perm = t->d_oidx[mode];
+        if (!perm) return fail(ALTOB_ERR_ARG, "OPSCHED needs oidx for the target mode (fiber reuse <= 4)");
+        break;
+    case ALTOB_ALGO_ATOMIC_CR:
+        return ft == ALTOB_F64 ? run_atomic_cr<double>(t, mode, dU, R, st) : run_atomic_cr<float>(t, mode, dU, R, st);
+    default: return fail(ALTOB_ERR_ARG, "unknown algorithm");
+    }
+    return ft == ALTOB_F64 ? run_tiled<double>(t, mode, dU, dU[mode], R, false, 0.0, perm, cache, st)
+                           : run_tiled<float>(t, mode, dU, dU[mode], R, false, 0.0, perm, cache, st);
+}
+
+altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, double eps,
+                        void* dphi, cudaStream_t st)
+{
+    if (!t || !dU || !dphi) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    if (ft != ALTOB_F64 && ft != ALTOB_F32) return fail(ALTOB_ERR_ARG, "compute dtype must be F64 or F32");
+    const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_CUDA(cudaMemsetAsync(dphi, 0, t->dims[mode] * R * fsz, st));
+    if (t->nnz == 0) return ALTOB_OK;
+    return ft == ALTOB_F64 ? run_tiled<double>(t, mode, dU, dphi, R, true, eps, nullptr, true, st)
+                           : run_tiled<float>(t, mode, dU, dphi, R, true, eps, nullptr, true, st);
+}
+
+// Copies host factors into the handle's cached scratch (no per-call
+// allocation once the scratch is large enough).
+static altob_status upload_factors(altob_tensor* t, void* const* h, size_t fsz, u64 R, void** d, cudaStream_t st)
+{
+    size_t total = 0, offs[ALTOB_MAX_MODES];
+    for (int m = 0; m < t->nmode; ++m) {
+        if (!h[m]) return fail(ALTOB_ERR_ARG, "a host factor pointer is NULL");
+        offs[m] = total;
+        total += (t->dims[m] * R * fsz + 255) & ~(size_t)255;
+    }
+    void* base = nullptr;
+    ALTOB_TRY(tensor_scratch(t, total, &base));
+    for (int m = 0; m < t->nmode; ++m) {
+        d[m] = (char*)base + offs[m];
+        ALTOB_CUDA(cudaMemcpyAsync(d[m], h[m], t->dims[m] * R * fsz, cudaMemcpyHostToDevice, st));
+    }
+    return ALTOB_OK;
+}
+
+}  // namespace altob
+
+using namespace altob;
+
+extern "C" {
+
+altob_status altob_mttkrp(altob_tensor* t, int mode, altob_dtype ftype, void* const* d_factors, uint64_t rank,
+                          int accumulate, altob_algo algo, void* stream)
+{
+    return mttkrp_device(t, mode, ftype, d_factors, rank, accumulate, algo, (cudaStream_t)stream);
+}
+
+altob_status altob_phi(altob_tensor* t, int mode, altob_dtype ftype, void* const* d_factors, uint64_t rank,
+                       double eps_div_zero, void* d_phi, void* stream)
+{
+    return phi_device(t, mode, ftype, d_factors, rank, eps_div_zero, d_phi, (cudaStream_t)stream);
+}
+
+altob_status altob_mttkrp_host(altob_tensor* t, int mode, altob_dtype ftype, void* const* h_factors, uint64_t rank,
+                               altob_algo algo, void* stream)
+{
+    if (!t || !h_factors) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
+    void* d[ALTOB_MAX_MODES];
+    altob_status s = upload_factors(t, h_factors, fsz, rank, d, st);
+    if (s == ALTOB_OK) s = mttkrp_device(t, mode, ftype, d, rank, 1, algo, st);
+    if (s == ALTOB_OK) {
+        cudaError_t e = cudaMemcpyAsync(h_factors[mode], d[mode], t->dims[mode] * rank * fsz,
+                                        cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("mttkrp_host: ") + cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(st);
+    return s;
+}
+
+altob_status altob_mttkrp_sweep_host(altob_tensor* t, altob_dtype ftype, void* const* h_factors, uint64_t rank,
+                                     int iters, altob_algo algo, void* stream)
+{
+    if (!t || !h_factors) return fail(ALTOB_ERR_ARG, "NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
+    void* d[ALTOB_MAX_MODES];
+    altob_status s = upload_factors(t, h_factors, fsz, rank, d, st);
+    for (int i = 0; i < iters && s == ALTOB_OK; ++i)
+        for (int m = 0; m < t->nmode && s == ALTOB_OK; ++m) s = mttkrp_device(t, m, ftype, d, rank, 1, algo, st);
+    for (int m = 0; m < t->nmode && s == ALTOB_OK; ++m) {
+        cudaError_t e = cudaMemcpyAsync(h_factors[m], d[m], t->dims[m] * rank * fsz, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep copy-out: ") + cudaGetErrorString(e));
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (s == ALTOB_OK && e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep: ") + cudaGetErrorString(e));
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,21 @@
+// mttkrp_plan.h -- host-side MTTKRP / Phi helpers shared by the solvers.
+#pragma once
+
+#include "internal.cuh"
+
+namespace altob {
+
+struct TiledPlan {
+    int vec, lpn, tile, hslots;
+    size_t smem;
+};
+
+bool ptr_aligned16(const void* p);
+altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, bool cache, TiledPlan* pl);
+altob_algo resolve_algo(const altob_tensor* t, int mode, altob_algo algo);
+altob_status mttkrp_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, int accumulate,
+                           altob_algo algo, cudaStream_t st);
+altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, double eps,
+                        void* dphi, cudaStream_t st);
+
+}  // namespace altob

@@ -1,0 +1,112 @@
+"""Seeded synthetic sparse tensors with the shapes and value distributions of
+the benchmark configurations (the reference measures on FROSTT tensors that
+are not available offline; these stand in for them).
+
+All generators are deterministic for a given seed and independent of the
+thread count.  They return (dims, cidx, vals) with cidx a (nmode, nnz)
+uint64 array (0-based) and vals float64.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def uniform_distinct(dims, nnz, seed, low=0.0):
+    """`nnz` distinct coordinates drawn uniformly without replacement;
+    values uniform in (0, 1] (config 1: 1000x800x600, 1M nonzeros)."""
+    dims = [int(d) for d in dims]
+    total = int(np.prod(np.array(dims, dtype=object)))
+    if nnz > total:
+        raise ValueError("more nonzeros than coordinates")
+    rng = np.random.default_rng(seed)
+    if total < 2**62:
+        picked = np.zeros(0, np.int64)
+        while picked.size < nnz:
+            need = int((nnz - picked.size) * 1.2) + 16
+            cand = rng.integers(0, total, size=need, dtype=np.int64)
+            picked = np.unique(np.concatenate([picked, cand]))
+        picked = rng.permutation(picked)[:nnz]
+        cidx = np.zeros((len(dims), nnz), np.uint64)
+        rem = picked.copy()
+        for n in range(len(dims) - 1, -1, -1):
+            cidx[n] = (rem % dims[n]).astype(np.uint64)
+            rem //= dims[n]
+    else:
+        cidx = np.stack([rng.integers(0, d, size=nnz * 2, dtype=np.int64) for d in dims]).astype(np.uint64)
+        _, first = np.unique(cidx.T, axis=0, return_index=True)
+        first = np.sort(first)[:nnz]
+        if first.size < nnz:
+            raise ValueError("could not draw enough distinct coordinates")
+        cidx = np.ascontiguousarray(cidx[:, first])
+    vals = 1.0 - rng.random(nnz)  # (0, 1]
+    return np.array(dims, np.uint64), cidx, vals
+
+
+def zipf_indices(rng, n, dim, s):
+    """`n` draws of a Zipf(s) distribution truncated to [1, dim], returned
+    0-based.  Draws above dim are redrawn (exact truncation)."""
+    out = rng.zipf(s, size=n)
+    bad = out > dim
+    while bad.any():
+        out[bad] = rng.zipf(s, size=int(bad.sum()))
+        bad = out > dim
+    return (out - 1).astype(np.uint64)
+
+
+def merge_duplicates(dims, cidx, vals):
+    """Sums values of repeated coordinates; output sorted lexicographically."""
+    nm = cidx.shape[0]
+    order = np.lexsort(cidx[::-1])
+    c = cidx[:, order]
+    v = vals[order]
+    if c.shape[1] == 0:
+        return c, v
+    new = np.ones(c.shape[1], bool)
+    new[1:] = np.any(c[:, 1:] != c[:, :-1], axis=0)
+    run = np.cumsum(new) - 1
+    out_v = np.zeros(int(new.sum()))
+    np.add.at(out_v, run, v)
+    return np.ascontiguousarray(c[:, new]), out_v
+
+
+def zipf_tensor(dims, draws, seed, s=1.1, lognormal=True):
+    """Config 2 shape: each mode index drawn independently from Zipf(s) over
+    its dimension, duplicates merged by summing, values log-normal(0, 1)."""
+    rng = np.random.default_rng(seed)
+    cidx = np.stack([zipf_indices(rng, draws, int(d), s) for d in dims])
+    vals = rng.lognormal(0.0, 1.0, size=draws) if lognormal else 1.0 - rng.random(draws)
+    cidx, vals = merge_duplicates(np.array(dims), cidx, vals)
+    return np.array(dims, np.uint64), cidx, vals
+
+
+def poisson_kruskal(dims, rank, total_counts, seed, shape=0.3, scale=1.0):
+    """Config 3 shape: Poisson counts from a Kruskal model with Gamma(shape,
+    scale) factor entries (columns normalised to probabilities, unit weights).
+    Each of `total_counts` events picks a component uniformly and then one
+    index per mode from that component's column; repeated coordinates are
+    merged into counts."""
+    rng = np.random.default_rng(seed)
+    nm = len(dims)
+    cols = []
+    for d in dims:
+        A = rng.gamma(shape, scale, size=(int(d), rank))
+        A /= A.sum(axis=0, keepdims=True)
+        cols.append(np.cumsum(A, axis=0))
+    comp = rng.integers(0, rank, size=total_counts)
+    cidx = np.zeros((nm, total_counts), np.uint64)
+    for n in range(nm):
+        u = rng.random(total_counts)
+        cdf = cols[n]
+        idx = np.empty(total_counts, np.int64)
+        for r in range(rank):
+            sel = comp == r
+            idx[sel] = np.searchsorted(cdf[:, r], u[sel], side="right")
+        cidx[n] = np.minimum(idx, int(dims[n]) - 1).astype(np.uint64)
+    cidx, vals = merge_duplicates(np.array(dims), cidx, np.ones(total_counts))
+    return np.array(dims, np.uint64), cidx, vals
+
+
+def random_factors(dims, rank, seed):
+    """Uniform(0,1) factor matrices from numpy (for parity inputs)."""
+    rng = np.random.default_rng(seed)
+    return [rng.random((int(d), rank)) for d in dims]

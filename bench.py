@@ -1,0 +1,429 @@
+#!/usr/bin/env python3
+"""Benchmark: MTTKRP along every mode of the large skewed tensor (FP32).
+
+Workload (one GPU): 3-mode tensor 4,800,000 x 1,800,000 x 1,800,000 built
+from 140,000,000 draws per mode of Zipf(s=1.1), duplicates merged by
+summing (about 100.9M nonzeros), values log-normal(0, 1) in FP32, 65 ALTO
+bits (128-bit index), rank 32.  Seeded synthetic data stands in for the
+FROSTT tensors the reference measures on.
+
+A step is one MTTKRP sweep: for every mode n the output matrix is zeroed and
+M_n = X_(n) (U_{others} Khatri-Rao) is computed by the ALTO kernel, the
+reference's mttkrp_alto_par sweep (src/main.cpp:476-495) with fixed inputs.
+
+  value  = nonzeros x modes / step time (device-resident inputs)   [Gnnz/s/mode]
+  e2e    = the same through the drop-in host call (altob_mttkrp_host: host
+           factors copied in, target copied back, every mode, every step)
+  roofline = algorithmic bytes of one MTTKRP launch / its CUDA-event time
+  cpu_baseline = the reference's OpenMP mttkrp_alto_par on a bounded sample
+
+--impl reference times the reference's own CPU implementation instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (4_800_000, 1_800_000, 1_800_000)
+DRAWS = 140_000_000
+RANK = 32
+ZIPF_S = 1.1
+SEED = 2
+METRIC = "mttkrp_gnnz_per_s_per_mode"
+UNIT = "Gnnz/s/mode"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="altob", choices=["altob", "reference"])
+    p.add_argument("--draws", type=int, default=DRAWS, help="Zipf draws per mode (smaller = profiling case)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-sample-draws", type=int, default=20_000_000)
+    p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
+    p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
+    return p.parse_args()
+
+
+# ------------------------------------------------------------ data (torch)
+
+def zipf_tensor_torch(dims, draws, s, seed, device):
+    """Config-2 tensor generated on the device: inverse-CDF Zipf draws per
+    mode, duplicate coordinates merged by summing log-normal values."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    idx = []
+    for d in dims:
+        k = torch.arange(1, d + 1, dtype=torch.float64, device=device)
+        cdf = torch.cumsum(k.pow(-s), 0)
+        cdf /= cdf[-1].clone()
+        u = torch.rand(draws, dtype=torch.float64, device=device, generator=g)
+        i = torch.searchsorted(cdf, u, right=True).clamp_(max=d - 1)
+        idx.append(i)
+        del k, cdf, u
+    vals = torch.exp(torch.randn(draws, dtype=torch.float64, device=device, generator=g))
+    low = idx[1] * dims[2] + idx[2]
+    o1 = torch.sort(low, stable=True).indices
+    o2 = torch.sort(idx[0][o1], stable=True).indices
+    order = o1[o2]
+    del o1, o2
+    i0, lo, v = idx[0][order], low[order], vals[order]
+    del idx, low, vals, order
+    new = torch.ones_like(i0, dtype=torch.bool)
+    new[1:] = (i0[1:] != i0[:-1]) | (lo[1:] != lo[:-1])
+    seg = torch.cumsum(new.to(torch.int64), 0) - 1
+    nnz = int(seg[-1].item()) + 1
+    vs = torch.zeros(nnz, dtype=torch.float64, device=device).index_add_(0, seg, v)
+    keep = new.nonzero().squeeze(1)
+    i0, lo = i0[keep], lo[keep]
+    cidx = torch.stack([i0, lo // dims[2], lo % dims[2]]).contiguous()
+    return cidx, vs.to(torch.float32), nnz
+
+
+# ------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples while the timed region runs."""
+
+    def __init__(self):
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", "0", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for p in self.samples:
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------- CPU baselines
+
+def reference_cpu_run(sample_file, iters):
+    """Runs the reference's mttkrp_alto_par sweep (oracle/_ref, or the oracle
+    port when the reference library is absent) on the sample; returns JSON."""
+    from oracle import orc
+    d = np.load(sample_file)
+    dims, cidx, vals = d["dims"], d["cidx"], d["vals"].astype(np.float64)
+    nnz = vals.shape[0]
+    cores = os.cpu_count()
+    if orc.ref_available():
+        ref = orc.RefLib()
+        cores = ref.max_threads()
+        t, create_s = ref.bench_mttkrp(dims, cidx, vals, cores, 128, RANK, iters, SEED)
+        kind = "reference"
+    else:
+        o = orc.Oracle()
+        at = o.create(dims, cidx, vals, 1, 128)
+        U = [np.random.default_rng(m).random((int(x), RANK)) for m, x in enumerate(dims)]
+        t0 = time.perf_counter()
+        for _ in range(iters):
+            for m in range(3):
+                at.mttkrp(m, U, RANK)
+        t = time.perf_counter() - t0
+        create_s = 0.0
+        kind, cores = "port", 1
+    value = nnz * 3 * iters / t / 1e9
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "seconds": t, "create_s": create_s,
+            "sample": f"{nnz} nonzeros ({int(d['draws'])} Zipf(1.1) draws per mode, same dims), rank {RANK}, "
+                      f"{iters} sweeps of mttkrp_alto_par over 3 modes, FP64, 128-bit ALTO index"}
+
+
+def make_cpu_sample(draws, path):
+    """Bounded sample of the workload: the same distribution with fewer
+    draws, written for the CPU process."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            cidx, vals, nnz = zipf_tensor_torch(DIMS, draws, ZIPF_S, SEED + 1000, "cuda")
+            np.savez(path, dims=np.array(DIMS, np.uint64), cidx=cidx.cpu().numpy().astype(np.uint64),
+                     vals=vals.cpu().numpy(), draws=np.int64(draws))
+            return
+    except ImportError:
+        pass
+    from alto_b200 import synth
+    dims, cidx, vals = synth.zipf_tensor(DIMS, draws, SEED + 1000, s=ZIPF_S)
+    np.savez(path, dims=dims, cidx=cidx, vals=vals.astype(np.float32), draws=np.int64(draws))
+
+
+def cpu_baseline(args):
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "sample.npz")
+        make_cpu_sample(args.cpu_sample_draws, path)
+        env = dict(os.environ)
+        env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        env["OMP_PROC_BIND"] = "close"
+        env["OMP_PLACES"] = "cores"
+        env["OPENBLAS_NUM_THREADS"] = "1"
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline-file", path, "--cpu-iters",
+                            str(args.cpu_iters)], env=env, capture_output=True, text=True, timeout=900)
+        line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not line:
+            return {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                    "sample": "failed: " + (r.stderr[-300:] if r.stderr else "no output")}
+        return json.loads(line[-1])
+
+
+# ------------------------------------------------------------ arms
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle import orc
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "sample.npz")
+        make_cpu_sample(args.cpu_sample_draws, path)
+        d = np.load(path)
+        dims, cidx, vals = d["dims"], d["cidx"], d["vals"].astype(np.float64)
+        nnz = vals.shape[0]
+        if orc.ref_available():
+            ref = orc.RefLib()
+            cores = ref.max_threads()
+            # each call: create_alto once (untimed by the reference itself),
+            # a warm-up sweep, then `steps` timed sweeps
+            t, _ = ref.bench_mttkrp(dims, cidx, vals, cores, 128, RANK, args.steps, SEED)
+            kind = "reference"
+        else:
+            o = orc.Oracle()
+            at = o.create(dims, cidx, vals, 1, 128)
+            U = [np.random.default_rng(m).random((int(x), RANK)) for m, x in enumerate(dims)]
+            for _ in range(args.warmup):
+                for m in range(3):
+                    at.mttkrp(m, U, RANK)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                for m in range(3):
+                    at.mttkrp(m, U, RANK)
+            t = time.perf_counter() - t0
+            kind, cores = "port", 1
+    value = nnz * 3 * args.steps / t / 1e9
+    sample = (f"{nnz} nonzeros from {args.cpu_sample_draws} Zipf(1.1) draws per mode over the same dims; "
+              f"each step one sweep of mttkrp_alto_par over 3 modes, rank {RANK}, FP64")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "mttkrp_sweep_zipf3_4.8Mx1.8Mx1.8M", "rank": RANK, "draws": args.cpu_sample_draws,
+                       "nnz": nnz, "alto_bits": 65},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_altob(args):
+    import torch
+    import alto_b200 as ab
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    # per-rank data: replicas of the workload with rank-dependent seeds (weak scaling)
+    cidx, vals, nnz = zipf_tensor_torch(DIMS, args.draws, ZIPF_S, SEED + 7919 * rank, dev)
+    at = ab.create_alto_device(3, np.array(DIMS, np.uint64), nnz, cidx, vals, nprtn=1024, lit_bits=128,
+                               val_dtype="f32", stream=stream)
+    del cidx, vals
+    torch.cuda.synchronize()
+    info = at.info()
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED)
+    U = [torch.rand(d, RANK, dtype=torch.float32, device=dev, generator=g) for d in DIMS]
+    out = [torch.zeros(d, RANK, dtype=torch.float32, device=dev) for d in DIMS]
+
+    def ptrs_for(n):
+        return [out[m] if m == n else U[m] for m in range(3)]
+
+    evs = [[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in range(3 * args.steps)]
+
+    def step(k=None):
+        for n in range(3):
+            out[n].zero_()
+            if k is not None:
+                evs[3 * k + n][0].record(stream)
+            ab.mttkrp_alto_par(n, ptrs_for(n), RANK, at, algo="auto", accumulate=True, stream=stream)
+            if k is not None:
+                evs[3 * k + n][1].record(stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    clk = ClockSampler()
+    clk.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    clocks = clk.stop()
+    if dist:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_step = ms / args.steps
+    value = ws * nnz * 3 / (ms_step / 1e3) / 1e9
+
+    # roofline of the MTTKRP kernel: algorithmic bytes per launch
+    kw_bytes = 16 if info["lit_bits"] == 128 else 8
+    stream_b = nnz * (kw_bytes + 4)
+    fac_b = [d * RANK * 4 for d in DIMS]
+    launch_ms = [[], [], []]
+    for k in range(args.steps):
+        for n in range(3):
+            launch_ms[n].append(evs[3 * k + n][0].elapsed_time(evs[3 * k + n][1]))
+    bytes_per_mode = [stream_b + sum(fac_b) for n in range(3)]  # other factors read once + output written once
+    avg_ms = [statistics.mean(x) for x in launch_ms]
+    achieved = sum(bytes_per_mode) / (sum(avg_ms) / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "mttkrp_traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as f:
+                tj = json.load(f)
+            traffic = tj.get("per_launch_bytes_full_size")
+        except (OSError, ValueError):
+            traffic = None
+
+    e2e = None
+    if not args.no_e2e:
+        hU = [torch.empty(d, RANK, dtype=torch.float32, pin_memory=True) for d in DIMS]
+        hO = [torch.zeros(d, RANK, dtype=torch.float32, pin_memory=True) for d in DIMS]
+        for h, u in zip(hU, U):
+            h.copy_(u.cpu())
+        hU_np = [h.numpy() for h in hU]
+        hO_np = [h.numpy() for h in hO]
+
+        def e2e_step():
+            for n in range(3):
+                facs = [hO_np[m] if m == n else hU_np[m] for m in range(3)]
+                ab.mttkrp_alto_par(n, facs, RANK, at, algo="auto", accumulate=True, stream=stream)
+
+        e2e_step()  # warm-up (also sizes the handle's scratch)
+        torch.cuda.synchronize()
+        ke = max(2, min(args.steps, 5))
+        tA = time.perf_counter()
+        for _ in range(ke):
+            e2e_step()
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - tA) / ke
+        h2d = 3 * sum(fac_b)
+        d2h = sum(fac_b)
+        e2e = {"value": ws * nnz * 3 / te / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": te * 1e3, "steps": ke,
+               "api": "altob_mttkrp_host (mttkrp_alto_par with host factors) for each mode"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and ws == 1:
+        del out
+        cpu = cpu_baseline(args)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "mttkrp_sweep_zipf3_4.8Mx1.8Mx1.8M" if args.draws == DRAWS else
+                           f"mttkrp_sweep_zipf3_small_{args.draws}", "dims": list(DIMS), "draws": args.draws,
+                           "nnz": nnz, "rank": RANK, "alto_bits": info["alto_bits"], "lit_bits": info["lit_bits"],
+                           "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (no flush)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                             "kernel": "k_tiled (MTTKRP)", "launch_ms_per_mode": avg_ms,
+                             "algorithmic_bytes_per_launch": bytes_per_mode},
+                "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.cpu_baseline_file:
+        print(json.dumps(reference_cpu_run(args.cpu_baseline_file, args.cpu_iters)), flush=True)
+        return 0
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_altob(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,232 @@
+/*
+ * altob.h -- C ABI of alto_b200, a B200-native (sm_100a) implementation of
+ * the ALTO hot path: linearized-tensor build, MTTKRP on every mode from one
+ * tensor copy, and the CP-ALS / CP-APR updates that consume it.
+ *
+ * Plain C types only: host pointers, device pointers (void*), sizes and a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Every
+ * entry point returns an altob_status; none asserts or exits.  A tensor
+ * handle is device resident, stream ordered, and must be used by one host
+ * thread at a time.
+ *
+ * Each declaration names the reference interface it replaces
+ * (IntelLabs/ALTO v0.1.2, file:line).
+ */
+#ifndef ALTOB_H_
+#define ALTOB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ALTOB_API __attribute__((visibility("default")))
+#else
+#define ALTOB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALTOB_MAX_MODES 5 /* config.mk:27 MAX_NUM_MODES */
+
+typedef enum {
+    ALTOB_OK = 0,
+    ALTOB_ERR_ARG = 1,         /* invalid argument */
+    ALTOB_ERR_BITS = 2,        /* ALTO bits exceed the index width (alto.hpp:709) */
+    ALTOB_ERR_CUDA = 3,        /* a CUDA runtime call or kernel failed */
+    ALTOB_ERR_NOMEM = 4,       /* device or host allocation failed */
+    ALTOB_ERR_IO = 5,          /* file missing or malformed */
+    ALTOB_ERR_UNSUPPORTED = 6, /* dtype / size combination not built */
+    ALTOB_ERR_NOT_FOUND = 7    /* no CUDA device */
+} altob_status;
+
+typedef enum {
+    ALTOB_F64 = 0, /* double (reference FType/ValType default, common.hpp:45-69) */
+    ALTOB_F32 = 1, /* float  (FP_TYPE32) */
+    ALTOB_U32 = 2  /* uint32 counts (VAL_TYPE_INT32), values only */
+} altob_dtype;
+
+/* MTTKRP conflict-resolution strategy.  AUTO follows the reference dispatch
+ * (alto.hpp:554-563): fiber reuse nnz/I_n > 4 -> TILED (the GPU form of
+ * da_mem_pull), else OPSCHED when oidx exists, else ATOMIC_CR / ATOMIC. */
+typedef enum {
+    ALTOB_ALGO_AUTO = 0,
+    ALTOB_ALGO_TILED = 1,     /* per-tile shared-memory row accumulators, atomic flush */
+    ALTOB_ALGO_ATOMIC = 2,    /* mttkrp_alto_atomic (alto.hpp:1030-1088) */
+    ALTOB_ALGO_ATOMIC_CR = 3, /* mttkrp_alto_atomic_cr (alto.hpp:1090-1158) */
+    ALTOB_ALGO_OPSCHED = 4    /* mttkrp_alto_op_sched (alto.hpp:1320-1415) */
+} altob_algo;
+
+typedef struct altob_tensor altob_tensor;
+
+/* Scalars and masks of an encoding (AltoTensor<LIT>, alto.hpp:27-54).
+ * 128-bit quantities are (lo, hi) word pairs. */
+typedef struct {
+    int nmode;
+    int nprtn;
+    int lit_bits;  /* 64 or 128 */
+    int alto_bits; /* popcount(alto_mask) */
+    int is_oidx;
+    int val_dtype; /* altob_dtype of the stored values */
+    uint64_t nnz;
+    uint64_t dims[ALTOB_MAX_MODES];
+    uint64_t mode_masks[ALTOB_MAX_MODES][2];
+    uint64_t cr_masks[ALTOB_MAX_MODES][2];
+    uint64_t alto_mask[2];
+    uint64_t alto_cr_mask[2];
+    uint64_t device_bytes; /* HBM held by the handle */
+} altob_info;
+
+/* COO tensor in host memory (SparseTensor, sptensor.hpp:8-25): cidx is
+ * mode-major SoA, cidx[n*nnz + i], 0-based; vals are FP64. */
+typedef struct {
+    int nmode;
+    uint64_t nnz;
+    uint64_t dims[ALTOB_MAX_MODES];
+    uint64_t* cidx;
+    double* vals;
+} altob_coo;
+
+ALTOB_API const char* altob_status_string(altob_status s);
+/* Text of the last error raised on the calling thread ("" if none). */
+ALTOB_API const char* altob_last_error(void);
+/* Library version string. */
+ALTOB_API const char* altob_version(void);
+
+/* ---- tensor build ------------------------------------------------------
+ * Replaces create_alto<LIT>(SparseTensor*, AltoTensor<LIT>**, int nprtn)
+ * (alto.hpp:108-294): packed LSB-first / shortest-first masks (:669-770),
+ * linearization (:184-202), sort (:772-803), oidx (:246-285), equal-nnz
+ * partitions, per-mode intervals and CR bits (:805-1028).  nprtn has the
+ * reference's meaning (it fixes prtn_ptr, intervals and the CR bits).
+ * lit_bits: 64, 128, or 0 = the smallest width that holds the ALTO bits.
+ * Host inputs; cidx as in altob_coo; vals in val_dtype. */
+ALTOB_API altob_status altob_create(int nmode, const uint64_t* dims, uint64_t nnz,
+                          const uint64_t* cidx, const void* vals,
+                          altob_dtype val_dtype, int nprtn, int lit_bits,
+                          void* stream, altob_tensor** out);
+
+/* Same, with cidx / vals already in device memory. */
+ALTOB_API altob_status altob_create_device(int nmode, const uint64_t* dims, uint64_t nnz,
+                                 const uint64_t* d_cidx, const void* d_vals,
+                                 altob_dtype val_dtype, int nprtn, int lit_bits,
+                                 void* stream, altob_tensor** out);
+
+/* Replaces destroy_alto (alto.hpp:296-322). */
+ALTOB_API altob_status altob_destroy(altob_tensor* t);
+
+ALTOB_API altob_status altob_get_info(const altob_tensor* t, altob_info* out);
+
+/* Copies the encoding back to the host in the reference's layout (for
+ * parity checks): idx as (lo, hi) words per nonzero, vals in the stored
+ * dtype, prtn_ptr[nprtn+1], intervals[nprtn*nmode] (start, stop) pairs
+ * (prtn_intervals, alto.hpp:42), oidx as nmode rows of nnz (rows of modes
+ * without oidx are left untouched).  Any output pointer may be NULL. */
+ALTOB_API altob_status altob_dump(const altob_tensor* t, uint64_t* idx, void* vals,
+                        uint64_t* prtn_ptr, uint64_t* intervals,
+                        uint64_t* oidx, void* stream);
+
+/* ---- MTTKRP ------------------------------------------------------------
+ * Replaces mttkrp_alto_par(int target_mode, FType** factors, IType rank,
+ * AltoTensor*, omp_lock_t*, FType** ofibs) (alto.hpp:617-623).
+ * d_factors: nmode device pointers, row-major I_n x rank in ftype.
+ * accumulate = 1 keeps the reference's += semantics; 0 overwrites. */
+ALTOB_API altob_status altob_mttkrp(altob_tensor* t, int mode, altob_dtype ftype,
+                          void* const* d_factors, uint64_t rank,
+                          int accumulate, altob_algo algo, void* stream);
+
+/* The same call with the factor matrices in HOST memory (the reference's
+ * calling convention): copies the factors in, runs, copies factors[mode]
+ * back.  Synchronous. */
+ALTOB_API altob_status altob_mttkrp_host(altob_tensor* t, int mode, altob_dtype ftype,
+                               void* const* h_factors, uint64_t rank,
+                               altob_algo algo, void* stream);
+
+/* `iters` sweeps of mttkrp over every mode with host factors, as the
+ * reference's benchmark loop (main.cpp:476-495): factors copied in once,
+ * += into each mode in turn, all factors copied back.  Synchronous. */
+ALTOB_API altob_status altob_mttkrp_sweep_host(altob_tensor* t, altob_dtype ftype,
+                                     void* const* h_factors, uint64_t rank,
+                                     int iters, altob_algo algo, void* stream);
+
+/* ---- CP-ALS ------------------------------------------------------------
+ * Replaces cpd_alto(AltoTensor*, KruskalModel*, int max_iters,
+ * double epsilon) (cpd.hpp:43-186).  d_factors / d_lambda (ftype) hold the
+ * initial model and receive the result.  fits[max_iters] (host, may be
+ * NULL) receives cpd_fit_alto (cpd.hpp:189-271) per iteration; *iters the
+ * number run.  The R x R Gram, solve, norms and fit run in FP64. */
+ALTOB_API altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype,
+                           void* const* d_factors, void* d_lambda,
+                           uint64_t rank, int max_iters, double epsilon,
+                           double* fits, int* iters, void* stream);
+
+/* cpd_alto's own calling convention: the model (factors, lambda) in HOST
+ * memory, copied to the device, solved, and copied back.  Synchronous. */
+ALTOB_API altob_status altob_cpd_als_host(altob_tensor* t, altob_dtype ftype,
+                                          void* const* h_factors, void* h_lambda,
+                                          uint64_t rank, int max_iters,
+                                          double epsilon, double* fits,
+                                          int* iters, void* stream);
+
+/* ---- CP-APR ------------------------------------------------------------
+ * Replaces cp_apr_alto(AltoTensor*, KruskalModel*, int max_iters,
+ * int max_inner_iters, FType epsilon, FType eps_div_zero, FType kappa_tol,
+ * FType kappa, bool dobench) (apr.hpp:984-1376).  summary[5] (host) =
+ * {log-likelihood, least-squares fit, final KKT violation, outer
+ * iterations, total inner iterations}.  KKT and log-likelihood in FP64. */
+ALTOB_API altob_status altob_cp_apr(altob_tensor* t, altob_dtype ftype,
+                          void* const* d_factors, void* d_lambda,
+                          uint64_t rank, int max_iters, int max_inner,
+                          double epsilon, double eps_div_zero,
+                          double kappa_tol, double kappa, int dobench,
+                          double* summary, void* stream);
+
+/* cp_apr_alto's calling convention: host model, copied in and out. */
+ALTOB_API altob_status altob_cp_apr_host(altob_tensor* t, altob_dtype ftype,
+                                         void* const* h_factors, void* h_lambda,
+                                         uint64_t rank, int max_iters,
+                                         int max_inner, double epsilon,
+                                         double eps_div_zero, double kappa_tol,
+                                         double kappa, int dobench,
+                                         double* summary, void* stream);
+
+/* Replaces CalculatePhi_alto_par (apr.hpp:297-303): d_phi (I_mode x rank,
+ * ftype) is overwritten; rows without nonzeros are 0. */
+ALTOB_API altob_status altob_phi(altob_tensor* t, int mode, altob_dtype ftype,
+                       void* const* d_factors, uint64_t rank,
+                       double eps_div_zero, void* d_phi, void* stream);
+
+/* Replaces tt_logLikelihood<LIT> (apr.hpp:851-982), including its
+ * redistribution of lambda into mode 0 and the 1-norm renormalisation. */
+ALTOB_API altob_status altob_loglik(altob_tensor* t, altob_dtype ftype,
+                          void* const* d_factors, void* d_lambda,
+                          uint64_t rank, double eps_div_zero,
+                          double* loglik, void* stream);
+
+/* ---- tensor files ------------------------------------------------------
+ * Replaces ImportSparseTensor (sptensor.cpp:165-258).  The .tns reader
+ * follows the reference (dims = largest index seen, '#' comments and empty
+ * lines skipped, 1-based unless zero_based) and parses in parallel. */
+ALTOB_API altob_status altob_read_tns(const char* path, int zero_based, altob_coo** out);
+/* Binary layout of sptensor.cpp:57-69 / 211-258: u64 nmodes, u64
+ * dims[nmodes], u64 nnz, nmodes x nnz u64 indices, nnz FP64 values. */
+ALTOB_API altob_status altob_read_bin(const char* path, altob_coo** out);
+ALTOB_API altob_status altob_write_bin(const char* path, const altob_coo* coo);
+/* Replaces ExportSparseTensor TEXT_FORMAT (sptensor.cpp:49-56). */
+ALTOB_API altob_status altob_write_tns(const char* path, const altob_coo* coo);
+ALTOB_API void altob_coo_free(altob_coo* coo);
+
+/* Replaces KruskalModelRandomInit (src/kruskal_model.cpp:109-125): lambda
+ * = 1 and U = (FType)rand() / RAND_MAX from glibc srand(seed), mode by mode,
+ * into host buffers (so a model initialised here equals the reference's). */
+ALTOB_API altob_status altob_kruskal_random_init(int nmode, const uint64_t* dims,
+                                                 uint64_t rank, unsigned seed,
+                                                 altob_dtype ftype,
+                                                 void* const* h_factors,
+                                                 void* h_lambda);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALTOB_H_ */

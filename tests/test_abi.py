@@ -1,0 +1,107 @@
+"""The C ABI library loads and exports every symbol include/altob.h
+declares; host-only entry points work without a GPU.  CPU only."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import alto_b200 as ab
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "altob.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"ALTOB_API[^;(]*?\b(altob_\w+)\s*\(", text, flags=re.S)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ab.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) == set(ab.SIGNATURES), "Python bindings and header disagree"
+
+
+def test_status_strings_and_version():
+    L = ab.lib()
+    assert L.altob_status_string(0) == b"ok"
+    assert b"argument" in L.altob_status_string(1)
+    assert b"sm_100a" in L.altob_version()
+
+
+def test_null_arguments_are_errors_not_crashes():
+    L = ab.lib()
+    assert L.altob_destroy(None) == 0
+    assert L.altob_get_info(None, None) == 1
+    assert L.altob_mttkrp(None, 0, 0, None, 8, 1, 0, None) == 1
+
+
+def test_tns_round_trip(tmp_path):
+    dims = np.array([4, 5, 6], np.uint64)
+    cidx = np.array([[0, 3, 1, 2], [4, 0, 2, 2], [5, 1, 0, 3]], np.uint64)
+    vals = np.array([1.5, -2.0, 3.25, 1e-3])
+    X = ab.SparseTensor.from_arrays(dims, cidx, vals)
+    p = str(tmp_path / "t.tns")
+    ab.ExportSparseTensor(p, ab.TEXT_FORMAT, X)
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.cidx, cidx)
+    np.testing.assert_allclose(Y.vals, vals)
+    np.testing.assert_array_equal(Y.dims, dims)  # dims = largest index seen
+
+
+def test_tns_reader_reference_rules(tmp_path):
+    # comments and empty lines skipped; dims from the largest index; tabs;
+    # 0-based reading with the reference's dims = max index + zero_based
+    p = str(tmp_path / "r.tns")
+    with open(p, "w") as f:
+        f.write("# a comment\n\n1 2 3 1.0\n4\t1 1 2.5\n\n2 2 7 -1e2\n")
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.dims, [4, 2, 7])
+    np.testing.assert_array_equal(Y.cidx, [[0, 3, 1], [1, 0, 1], [2, 0, 6]])
+    np.testing.assert_allclose(Y.vals, [1.0, 2.5, -100.0])
+    Z = ab.ImportSparseTensor(p, ab.TEXT_FORMAT, zero_based=1)
+    np.testing.assert_array_equal(Z.dims, [5, 3, 8])
+    np.testing.assert_array_equal(Z.cidx, [[1, 4, 2], [2, 1, 2], [3, 1, 7]])
+
+
+def test_tns_reader_large_parallel(tmp_path):
+    from alto_b200 import synth
+    dims, cidx, vals = synth.uniform_distinct((300, 200, 100), 200_000, seed=2)
+    X = ab.SparseTensor.from_arrays(dims, cidx, vals)
+    p = str(tmp_path / "big.tns")
+    ab.ExportSparseTensor(p, ab.TEXT_FORMAT, X)
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.cidx, cidx)
+    np.testing.assert_allclose(Y.vals, vals, rtol=1e-5)  # %g keeps 6 digits
+
+
+def test_binary_round_trip_and_errors(tmp_path):
+    dims = np.array([7, 8], np.uint64)
+    cidx = np.array([[1, 6], [7, 0]], np.uint64)
+    vals = np.array([0.5, 0.25])
+    X = ab.SparseTensor.from_arrays(dims, cidx, vals)
+    p = str(tmp_path / "t.bin")
+    ab.ExportSparseTensor(p, ab.BINARY_FORMAT, X)
+    Y = ab.ImportSparseTensor(p, ab.BINARY_FORMAT)
+    np.testing.assert_array_equal(Y.cidx, cidx)
+    np.testing.assert_array_equal(Y.vals, vals)
+    with open(p, "r+b") as f:
+        f.truncate(40)
+    with pytest.raises(ab.AltobError) as e:
+        ab.ImportSparseTensor(p, ab.BINARY_FORMAT)
+    assert e.value.status == 5
+    with pytest.raises(ab.AltobError):
+        ab.ImportSparseTensor(str(tmp_path / "missing.tns"))
+
+
+def test_random_init_matches_glibc_reference_stream(oracle):
+    M = ab.random_init_factors([30, 20, 10], 7, 1234)
+    U, lam = oracle.random_init([30, 20, 10], 7, 1234)
+    for a, b in zip(M.U, U):
+        np.testing.assert_array_equal(a, b)
+    M32 = ab.random_init_factors([30, 20, 10], 7, 1234, dtype=np.float32)
+    np.testing.assert_allclose(M32.U[2], U[2].astype(np.float32), rtol=1e-7)

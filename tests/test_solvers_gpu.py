@@ -1,0 +1,136 @@
+"""CP-ALS and CP-APR on the GPU against fixtures written by the reference
+and against the oracle.  Fit and log-likelihood tolerance: 1e-4 (FP32
+model against the FP64 reference); FP64 runs are held much tighter."""
+import numpy as np
+import pytest
+
+import alto_b200 as ab
+from alto_b200 import synth
+from conftest import load_golden, rel_fro
+
+pytestmark = pytest.mark.gpu
+
+
+def _coo(dims, cidx, vals):
+    return ab.SparseTensor.from_arrays(dims, cidx, vals)
+
+
+def test_gpu_cpd_fp64_matches_reference_fixture():
+    g = load_golden("cpd_u3")
+    rank = int(g["rank"])
+    at = ab.create_alto(_coo(g["dims"], g["cidx"], g["vals"]), int(g["nprtn"]), 64)
+    M = ab.random_init_factors(g["dims"], rank, int(g["seed"]))
+    fits = ab.cpd_alto(at, M, int(g["max_iters"]), 1e-30)
+    assert len(fits) == len(g["fits"])
+    np.testing.assert_allclose(fits, g["fits"], rtol=2e-6)  # printed with %g
+    for n in range(3):
+        assert rel_fro(M.U[n], g[f"U{n}"]) < 1e-8
+    np.testing.assert_allclose(M.lam, g["lam"], rtol=1e-8)
+
+
+def test_gpu_cpd_fp64_stopping_rule_matches_reference():
+    g = load_golden("cpd_conv4")
+    rank = int(g["rank"])
+    at = ab.create_alto(_coo(g["dims"], g["cidx"], g["vals"]), int(g["nprtn"]), 64)
+    M = ab.random_init_factors(g["dims"], rank, int(g["seed"]))
+    fits = ab.cpd_alto(at, M, int(g["max_iters"]), float(g["eps"]))
+    assert len(fits) == len(g["fits"])
+    np.testing.assert_allclose(fits, g["fits"], rtol=2e-6)
+
+
+def test_gpu_cpd_config1_fp64_and_fp32_fit_trajectory():
+    """Config 1 (1000x800x600, 1M nonzeros, rank 16, 20 iterations): FP64
+    and FP32 fits against the reference's printed trajectory."""
+    ref = load_golden("cpd_config1_fits")
+    dims, cidx, vals = synth.uniform_distinct((1000, 800, 600), 1_000_000, seed=int(ref["data_seed"]))
+    at = ab.create_alto(_coo(dims, cidx, vals), int(ref["nprtn"]), 64)
+    M = ab.random_init_factors(dims, 16, int(ref["seed"]))
+    fits = ab.cpd_alto(at, M, 20, 1e-30)
+    assert len(fits) == 20
+    assert np.max(np.abs(fits - ref["fits"])) < 1e-7
+    at32 = ab.create_alto(_coo(dims, cidx, vals), int(ref["nprtn"]), 64, val_dtype="f32")
+    M32 = ab.random_init_factors(dims, 16, int(ref["seed"]), dtype=np.float32)
+    fits32 = ab.cpd_alto(at32, M32, 20, 1e-30)
+    assert np.max(np.abs(fits32 - ref["fits"])) < 1e-4
+
+
+def test_gpu_cpd_device_model_matches_oracle(oracle):
+    torch = pytest.importorskip("torch")
+    dims, cidx, vals = synth.uniform_distinct((300, 200, 100, 50), 100_000, seed=5)
+    rank = 24
+    at = ab.create_alto(_coo(dims, cidx, vals), 16, 0)
+    U, lam = oracle.random_init(dims, rank, 3)
+    ot = oracle.create(dims, cidx, vals, 16, 64)
+    dU = [torch.from_numpy(u.copy()).cuda() for u in U]
+    dl = torch.from_numpy(lam.copy()).cuda()
+    M = ab.KruskalModel([int(d) for d in dims], rank, dU, dl)
+    fits = ab.cpd_alto(at, M, 8, 1e-30)
+    ofits = ot.cpd_als(U, lam, rank, 8, 1e-30)
+    np.testing.assert_allclose(fits, ofits, rtol=1e-9)
+    for n in range(4):
+        assert rel_fro(dU[n].cpu().numpy(), U[n]) < 1e-8
+
+
+@pytest.mark.parametrize("name", ["apr_bench", "apr_eps"])
+def test_gpu_cp_apr_fp64_matches_reference_fixture(name):
+    g = load_golden(name)
+    rank = int(g["rank"])
+    at = ab.create_alto(_coo(g["dims"], g["cidx"], g["vals"]), int(g["nprtn"]), 64, val_dtype="u32")
+    M = ab.random_init_factors(g["dims"], rank, int(g["seed"]))
+    r = ab.cp_apr_alto(at, M, int(g["max_iters"]), int(g["max_inner"]), float(g["eps"]), 1e-10, 1e-10, 1e-2,
+                       bool(g["dobench"]))
+    assert r["outer"] == int(g["outer"]) and r["inner"] == int(g["inner"])
+    np.testing.assert_allclose(r["loglik"], g["loglik"], rtol=1e-6)
+    np.testing.assert_allclose(r["fit"], g["fit"], rtol=1e-6)
+    np.testing.assert_allclose(r["kkt"], g["kkt"], rtol=1e-6)
+    for n in range(3):
+        assert rel_fro(M.U[n], g[f"U{n}"]) < 1e-8
+
+
+def test_gpu_cp_apr_early_exit_and_fp32(oracle):
+    dims, cidx, vals = synth.poisson_kruskal((200, 150, 100, 20), 6, 200_000, seed=6)
+    rank = 8
+    U, lam = oracle.random_init(dims, rank, 4)
+    ot = oracle.create(dims, cidx, vals, 8, 64)
+    oU = [u.copy() for u in U]
+    olam = lam.copy()
+    want = ot.cp_apr(oU, olam, rank, 12, 10, eps=1e-2)
+    at = ab.create_alto(_coo(dims, cidx, vals), 8, 0, val_dtype="u32")
+    M = ab.KruskalModel([int(d) for d in dims], rank, [u.copy() for u in U], lam.copy())
+    got = ab.cp_apr_alto(at, M, 12, 10, epsilon=1e-2)
+    assert got["outer"] == want["outer"] and got["inner"] == want["inner"]
+    np.testing.assert_allclose(got["loglik"], want["loglik"], rtol=1e-9)
+    np.testing.assert_allclose(got["fit"], want["fit"], rtol=1e-8, atol=1e-10)
+    # FP32 model, bench mode (fixed inner counts), against the FP64 oracle
+    oU = [u.copy() for u in U]
+    olam = lam.copy()
+    want = ot.cp_apr(oU, olam, rank, 6, 5, eps=0.0, dobench=True)
+    M32 = ab.KruskalModel([int(d) for d in dims], rank, [u.astype(np.float32) for u in U], lam.astype(np.float32))
+    got = ab.cp_apr_alto(at, M32, 6, 5, epsilon=0.0, dobench=True)
+    assert abs(got["loglik"] - want["loglik"]) <= 1e-4 * abs(want["loglik"])
+    assert abs(got["fit"] - want["fit"]) <= 1e-4
+
+
+def test_gpu_phi_and_loglik_match_oracle(oracle):
+    torch = pytest.importorskip("torch")
+    dims, cidx, vals = synth.poisson_kruskal((120, 90, 60), 5, 50_000, seed=8)
+    rank = 12
+    at = ab.create_alto(_coo(dims, cidx, vals), 4, 0, val_dtype="u32")
+    ot = oracle.create(dims, cidx, vals, 4, 64)
+    U = synth.random_factors(dims, rank, seed=9)
+    dU = [torch.from_numpy(u).cuda() for u in U]
+    for mode in range(3):
+        want = ot.phi(mode, U, rank)
+        phi = torch.empty(int(dims[mode]), rank, dtype=torch.float64, device="cuda")
+        ab.calculate_phi(at, mode, dU, rank, phi)
+        assert rel_fro(phi.cpu().numpy(), want) < 1e-12
+    lam = np.linspace(0.5, 2.0, rank)
+    oU = [u.copy() for u in U]
+    olam = lam.copy()
+    want = ot.loglik(oU, olam, rank)
+    dl = torch.from_numpy(lam.copy()).cuda()
+    M = ab.KruskalModel([int(d) for d in dims], rank, dU, dl)
+    got = ab.tt_logLikelihood(at, M)
+    np.testing.assert_allclose(got, want, rtol=1e-12)
+    assert rel_fro(dU[0].cpu().numpy(), oU[0]) < 1e-13
+    np.testing.assert_allclose(dl.cpu().numpy(), olam, rtol=1e-12)
