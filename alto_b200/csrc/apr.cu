@@ -51,28 +51,27 @@ __global__ void k_kappa(FT* __restrict__ B, const FT* __restrict__ Phi, u64 n, d
 
 template <typename FT>
 struct LLArgs {
-    const u64* klo;
-    const u64* khi;
+    KeySrc key;
     const void* vals;
     u64 nnz;
     int nmode, R;
     double eps;
     const FT* U[ALTOB_MAX_MODES];
-    Decoder dec;
+    Fields fld;
 };
 
 // sum_nnz v * log(max(sum_r prod_n U_n[i_n, r], eps)) (apr.hpp:913-943).
-template <typename FT, typename VT, int KW>
+template <typename FT, typename VT>
 __global__ void __launch_bounds__(256) k_loglik(LLArgs<FT> a, double* __restrict__ acc)
 {
     const VT* vals = reinterpret_cast<const VT*>(a.vals);
     double s = 0.0;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.nnz; i += (u64)gridDim.x * blockDim.x) {
-        u32 w[4];
-        split_key(a.klo[i], KW == 2 ? a.khi[i] : 0ull, w);
+        const u64 lo = a.key.klo[i], hi = key_hi(a.key, i);
         const FT* rows[ALTOB_MAX_MODES];
-        for (int m = 0; m < a.nmode; ++m)
-            rows[m] = a.U[m] + (size_t)decode_mode(w, a.dec.md[m], a.dec.nwords) * a.R;
+#pragma unroll
+        for (int m = 0; m < ALTOB_MAX_MODES; ++m)
+            if (m < a.nmode) rows[m] = a.U[m] + (size_t)field(lo, hi, a.fld.pos[m], a.fld.mask[m]) * a.R;
         double tmp = 0.0;
         for (int r = 0; r < a.R; ++r) {
             double p = 1.0;
@@ -99,21 +98,16 @@ static altob_status loglik_sum(const altob_tensor* t, FT** U, int R, double eps,
     if (t->nnz == 0) return ALTOB_OK;
     LLArgs<FT> a;
     memset(&a, 0, sizeof(a));
-    a.klo = t->d_klo;
-    a.khi = t->d_khi;
+    a.key = key_src(t);
     a.vals = t->d_vals;
     a.nnz = t->nnz;
     a.nmode = t->nmode;
     a.R = R;
     a.eps = eps;
     for (int m = 0; m < t->nmode; ++m) a.U[m] = U[m];
-    a.dec = t->dec;
+    a.fld = t->fld;
     const int g = ew_grid(t->nnz);
-#define LLK(VT)                                                                      \
-    do {                                                                             \
-        if (t->kw == 2) k_loglik<FT, VT, 2><<<g, 256, 0, st>>>(a, acc);              \
-        else k_loglik<FT, VT, 1><<<g, 256, 0, st>>>(a, acc);                         \
-    } while (0)
+#define LLK(VT) k_loglik<FT, VT><<<g, 256, 0, st>>>(a, acc)
     if (t->vdt == ALTOB_U32) LLK(u32);
     else if (t->vdt == ALTOB_F64) LLK(double);
     else LLK(float);
@@ -328,3 +322,4 @@ altob_status altob_loglik(altob_tensor* t, altob_dtype ftype, void* const* d_fac
 }
 
 }  // extern "C"
+

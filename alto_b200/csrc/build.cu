@@ -83,9 +83,9 @@ static int mode_bits(u64 d) { return d <= 1 ? 0 : 64 - __builtin_clzll(d - 1); }
 // setup_packed_alto(LSB_FIRST, SHORT_FIRST), alto.hpp:669-770: modes in
 // ascending bit count (ties in mode order), one bit per mode per level,
 // starting at the least significant bit.
-static int make_masks(int nmode, const u64* dims, u128* masks)
+static int make_masks(int nmode, const u64* dims, u128* masks, int* order)
 {
-    int bits[ALTOB_MAX_MODES], order[ALTOB_MAX_MODES], total = 0;
+    int bits[ALTOB_MAX_MODES], total = 0;
     for (int n = 0; n < nmode; ++n) {
         bits[n] = mode_bits(dims[n]);
         order[n] = n;
@@ -401,21 +401,60 @@ __global__ void k_gather_vals(const VI* __restrict__ in, const u32* __restrict__
         out[i] = (VO)in[perm[i]];
 }
 
-__device__ __forceinline__ void load_key(const u64* klo, const u64* khi, int kw, u64 i, u32 w[4])
-{
-    u64 lo = klo[i];
-    u64 hi = kw == 2 ? khi[i] : 0;
-    split_key(lo, hi, w);
-}
-
-// Mode indices of sorted keys (for the oidx sort).
-__global__ void k_mode_keys(const u64* __restrict__ klo, const u64* __restrict__ khi, int kw, u64 n, Decoder dec,
-                            int mode, u64* __restrict__ out, u32* __restrict__ iota)
+// Interleaved ALTO key -> field layout (same sort order).  CR bits are not
+// set yet at this point.
+__global__ void k_reencode(u64* __restrict__ klo, u64* __restrict__ khi, int kw, u64 n, Decoder dec, Fields f)
 {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
         u32 w[4];
-        load_key(klo, khi, kw, i, w);
-        out[i] = decode_mode(w, dec.md[mode], dec.nwords);
+        split_key(klo[i], kw == 2 ? khi[i] : 0ull, w);
+        u64 lo = 0, hi = 0;
+        for (int m = 0; m < dec.nmode; ++m) {
+            const u64 c = decode_mode(w, dec.md[m], dec.nwords);
+            const u32 p = f.pos[m];
+            if (p < 64) {
+                lo |= c << p;
+                if (p > 0 && p + 32 > 64) hi |= c >> (64 - p);
+            } else {
+                hi |= c << (p - 64);
+            }
+        }
+        klo[i] = lo;
+        if (kw == 2) khi[i] = hi;
+    }
+}
+
+// Field layout -> interleaved ALTO key (for altob_dump); bits at and above
+// alto_bits (the CR bits) are copied unchanged.
+__global__ void k_interleave(const u64* __restrict__ klo, KeySrc ks, int alto_bits, u64 n, Decoder dec, Fields f,
+                             u64* __restrict__ olo, u64* __restrict__ ohi)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 lo = klo[i], hi = key_hi(ks, i);
+        u32 w[4] = {0, 0, 0, 0};
+        for (int m = 0; m < dec.nmode; ++m) {
+            const u32 c = field(lo, hi, f.pos[m], f.mask[m]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const WordDec& wd = dec.md[m].w[q];
+                if (q < dec.nwords && wd.m) w[q] |= expand32(c >> wd.off, wd);
+            }
+        }
+        u64 ilo = (u64)w[0] | ((u64)w[1] << 32), ihi = (u64)w[2] | ((u64)w[3] << 32);
+        if (alto_bits < 64) ilo |= lo & (~0ull << alto_bits);
+        if (alto_bits <= 64) ihi |= hi;  // every high bit is a CR bit
+        else ihi |= hi & (~0ull << (alto_bits - 64));
+        olo[i] = ilo;
+        ohi[i] = ihi;
+    }
+}
+
+// Mode indices of the sorted keys (for the oidx sort).
+__global__ void k_mode_keys(const u64* __restrict__ klo, const u64* __restrict__ khi, u64 n, Fields f, int mode,
+                            u64* __restrict__ out, u32* __restrict__ iota)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        out[i] = field(klo[i], khi ? khi[i] : 0ull, f.pos[mode], f.mask[mode]);
         iota[i] = (u32)i;
     }
 }
@@ -432,8 +471,8 @@ __global__ void k_init_intervals(u64* iv, int nprtn, int nmode, u64 d0, u64 d1, 
 
 // Per-partition min / max of every mode index (prtn_alto, alto.hpp:874-899).
 // A warp whose 32 keys lie in one partition reduces in registers first.
-__global__ void k_intervals(const u64* __restrict__ klo, const u64* __restrict__ khi, int kw, u64 n, Decoder dec,
-                            u64 per, u64* __restrict__ iv)
+__global__ void k_intervals(const u64* __restrict__ klo, const u64* __restrict__ khi, u64 n, Fields f, u64 per,
+                            u64* __restrict__ iv)
 {
     const int lane = threadIdx.x & 31;
     const u64 stride = (u64)gridDim.x * blockDim.x;
@@ -444,10 +483,9 @@ __global__ void k_intervals(const u64* __restrict__ klo, const u64* __restrict__
         u64 p0 = __shfl_sync(0xffffffffu, p, 0);
         u64 pl = __shfl_sync(0xffffffffu, p, 31);
         bool uniform = (p0 == pl) || (base + 31 >= n && __all_sync(0xffffffffu, !valid || p == p0));
-        u32 w[4] = {0, 0, 0, 0};
-        if (valid) load_key(klo, khi, kw, i, w);
-        for (int m = 0; m < dec.nmode; ++m) {
-            u32 c = valid ? decode_mode(w, dec.md[m], dec.nwords) : 0;
+        u64 lo = valid ? klo[i] : 0, hi = (valid && khi) ? khi[i] : 0;
+        for (int m = 0; m < f.nmode; ++m) {
+            u32 c = valid ? field(lo, hi, f.pos[m], f.mask[m]) : 0;
             if (uniform) {
                 u32 mn = valid ? c : 0xffffffffu, mx = valid ? c : 0;
 #pragma unroll
@@ -456,12 +494,12 @@ __global__ void k_intervals(const u64* __restrict__ klo, const u64* __restrict__
                     mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
                 }
                 if (lane == 0) {
-                    u64* e = iv + (p0 * dec.nmode + m) * 2;
+                    u64* e = iv + (p0 * f.nmode + m) * 2;
                     atomicMin((unsigned long long*)e, (unsigned long long)mn);
                     atomicMax((unsigned long long*)(e + 1), (unsigned long long)mx);
                 }
             } else if (valid) {
-                u64* e = iv + (p * dec.nmode + m) * 2;
+                u64* e = iv + (p * f.nmode + m) * 2;
                 atomicMin((unsigned long long*)e, (unsigned long long)c);
                 atomicMax((unsigned long long*)(e + 1), (unsigned long long)c);
             }
@@ -475,16 +513,15 @@ struct CrArgs {
 };
 
 // Fiber ownership (alto.hpp:970-996): 0 untouched, p+1 one partition, -1 shared.
-__global__ void k_cr_owner(const u64* __restrict__ klo, const u64* __restrict__ khi, int kw, u64 n, Decoder dec,
-                           u64 per, CrArgs a)
+__global__ void k_cr_owner(const u64* __restrict__ klo, const u64* __restrict__ khi, u64 n, Fields f, u64 per,
+                           CrArgs a)
 {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        u32 w[4];
-        load_key(klo, khi, kw, i, w);
+        const u64 lo = klo[i], hi = khi ? khi[i] : 0;
         int p1 = (int)(i / per) + 1;
-        for (int m = 0; m < dec.nmode; ++m) {
+        for (int m = 0; m < f.nmode; ++m) {
             if (a.bitpos[m] < 0) continue;
-            u32 c = decode_mode(w, dec.md[m], dec.nwords);
+            u32 c = field(lo, hi, f.pos[m], f.mask[m]);
             int old = atomicCAS(&a.owner[m][c], 0, p1);
             if (old != 0 && old != p1 && old != -1) atomicExch(&a.owner[m][c], -1);
         }
@@ -492,24 +529,42 @@ __global__ void k_cr_owner(const u64* __restrict__ klo, const u64* __restrict__ 
 }
 
 // Sets the CR bits of nonzeros whose fiber is shared (alto.hpp:998-1019).
-__global__ void k_cr_set(u64* __restrict__ klo, u64* __restrict__ khi, int kw, u64 n, Decoder dec, CrArgs a)
+__global__ void k_cr_set(u64* __restrict__ klo, u64* __restrict__ khi, u64 n, Fields f, CrArgs a)
 {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        u32 w[4];
-        load_key(klo, khi, kw, i, w);
+        const u64 lo = klo[i], hi = khi ? khi[i] : 0;
         u64 add_lo = 0, add_hi = 0;
-        for (int m = 0; m < dec.nmode; ++m) {
+        for (int m = 0; m < f.nmode; ++m) {
             int b = a.bitpos[m];
             if (b < 0) continue;
-            u32 c = decode_mode(w, dec.md[m], dec.nwords);
+            u32 c = field(lo, hi, f.pos[m], f.mask[m]);
             if (a.owner[m][c] == -1) {
                 if (b < 64) add_lo |= 1ull << b;
                 else add_hi |= 1ull << (b - 64);
             }
         }
-        if (add_lo) klo[i] |= add_lo;
-        if (add_hi && kw == 2) khi[i] |= add_hi;
+        if (add_lo) klo[i] = lo | add_lo;
+        if (add_hi && khi) khi[i] = hi | add_hi;
     }
+}
+
+// Positions where the high key word changes (for the run table) and a
+// check that it never decreases.
+__global__ void k_hi_runs(const u64* __restrict__ khi, u64 n, u64* __restrict__ starts, u32 cap,
+                          u32* __restrict__ count, u32* __restrict__ decreasing)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        if (i == 0 || khi[i] != khi[i - 1]) {
+            if (i > 0 && khi[i] < khi[i - 1]) atomicExch(decreasing, 1u);
+            u32 k = atomicAdd(count, 1u);
+            if (k < cap) starts[k] = i;
+        }
+    }
+}
+
+__global__ void k_gather_u64(const u64* __restrict__ src, const u64* __restrict__ idx, u32 n, u64* __restrict__ out)
+{
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = src[idx[i]];
 }
 
 static int grid_for(u64 n, int threads)
@@ -578,6 +633,11 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
         std::swap(khi, khi2);
         std::swap(perm, perm2);
     }
+    // interleaved -> field layout (same order)
+    if (nnz) {
+        k_reencode<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, kw, nnz, t->dec, t->fld);
+        if (cudaGetLastError() != cudaSuccess) BTRY(fail(ALTOB_ERR_CUDA, "k_reencode launch failed"));
+    }
     // values in sorted order, converted to the stored dtype
     size_t vsz = val_size(t->vdt);
     BTRY(dmalloc(&t->d_vals, nnz * vsz + 16));
@@ -614,7 +674,7 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
                 cleanup();
                 return s;
             }
-            k_mode_keys<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, kw, nnz, t->dec, n, mk, perm2);
+            k_mode_keys<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, nnz, t->fld, n, mk, perm2);
             bool alt2 = false;
             s = radix_sort_pairs(mk, nullptr, perm2, mk2, nullptr, ox2, nnz, 1, mode_bits(t->dims[n]), st, &alt2);
             dfree(mk2);
@@ -640,7 +700,7 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
     u64* d_iv = nullptr;
     BTRY(dmalloc_t(&d_iv, (u64)np * nm * 2));
     k_init_intervals<<<(np * nm + 255) / 256, 256, 0, st>>>(d_iv, np, nm, dm[0], dm[1], dm[2], dm[3], dm[4]);
-    if (nnz) k_intervals<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, kw, nnz, t->dec, per, d_iv);
+    if (nnz) k_intervals<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, nnz, t->fld, per, d_iv);
     t->intervals.assign((size_t)np * nm * 2, 0);
     cudaMemcpyAsync(t->intervals.data(), d_iv, t->intervals.size() * sizeof(u64), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
@@ -673,8 +733,8 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
             if (s != ALTOB_OK) break;
         }
         if (s == ALTOB_OK) {
-            k_cr_owner<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, kw, nnz, t->dec, per, ca);
-            k_cr_set<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, kw, nnz, t->dec, ca);
+            k_cr_owner<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, nnz, t->fld, per, ca);
+            k_cr_set<<<grid_for(nnz, 256), 256, 0, st>>>(klo, khi, nnz, t->fld, ca);
             e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("CR bits: ") + cudaGetErrorString(e));
         }
@@ -684,11 +744,59 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
             return s;
         }
     }
+    // high key words: a run table when they never decrease along the stream
+    // (the usual case: they are the top ALTO bits), else one word per nonzero
+    if (kw == 2 && nnz) {
+        const u32 cap = 1u << 16;
+        u64* starts = nullptr;
+        u32* cnt = nullptr;
+        BTRY(dmalloc_t(&starts, cap));
+        s = dmalloc_t(&cnt, 2);
+        if (s != ALTOB_OK) {
+            dfree(starts);
+            cleanup();
+            return s;
+        }
+        cudaMemsetAsync(cnt, 0, 2 * sizeof(u32), st);
+        k_hi_runs<<<grid_for(nnz, 256), 256, 0, st>>>(khi, nnz, starts, cap, cnt, cnt + 1);
+        u32 hc[2] = {0, 0};
+        cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && hc[1] == 0 && hc[0] <= cap) {
+            std::vector<u64> hs(hc[0]);
+            cudaMemcpy(hs.data(), starts, hc[0] * sizeof(u64), cudaMemcpyDeviceToHost);
+            std::sort(hs.begin(), hs.end());
+            u64 *rs = nullptr, *rv = nullptr;
+            s = dmalloc_t(&rs, hc[0]);
+            if (s == ALTOB_OK) s = dmalloc_t(&rv, hc[0]);
+            if (s == ALTOB_OK) {
+                cudaMemcpy(rs, hs.data(), hc[0] * sizeof(u64), cudaMemcpyHostToDevice);
+                k_gather_u64<<<std::max(1u, (hc[0] + 255) / 256), 256, 0, st>>>(khi, rs, hc[0], rv);
+                e = cudaStreamSynchronize(st);
+                if (e == cudaSuccess) {
+                    t->d_run_start = rs;
+                    t->d_run_val = rv;
+                    t->nrun = (int)hc[0];
+                    dfree(khi);
+                    khi = nullptr;
+                } else {
+                    dfree(rs);
+                    dfree(rv);
+                }
+            } else {
+                dfree(rs);
+            }
+        }
+        dfree(starts);
+        dfree(cnt);
+        if (e != cudaSuccess) BTRY(fail(ALTOB_ERR_CUDA, std::string("high-word runs: ") + cudaGetErrorString(e)));
+        if (s != ALTOB_OK) BTRY(s);
+    }
     t->d_klo = klo;
     t->d_khi = khi;
     cleanup();
 #undef BTRY
-    t->device_bytes = nnz * (8 * kw + vsz);
+    t->device_bytes = nnz * (8 * (khi ? 2 : 1) + vsz) + (u64)t->nrun * 16;
     for (int n = 0; n < nm; ++n)
         if (t->d_oidx[n]) t->device_bytes += nnz * 4;
     return ALTOB_OK;
@@ -716,7 +824,7 @@ static altob_status create_common(int nmode, const u64* dims, u64 nnz, const u64
     t->nnz = nnz;
     t->vdt = vdt;
     for (int n = 0; n < nmode; ++n) t->dims[n] = dims[n];
-    int total = make_masks(nmode, dims, t->masks);
+    int total = make_masks(nmode, dims, t->masks, t->order);
     if (lit_bits == 0) lit_bits = total <= 64 ? 64 : 128;
     if (total > lit_bits) {
         delete t;
@@ -735,6 +843,17 @@ static altob_status create_common(int nmode, const u64* dims, u64 nnz, const u64
         }
     t->kw = (total + ncr > 64) ? 2 : 1;
     t->dec = make_decoder(nmode, t->masks, total);
+    t->fld.nmode = nmode;
+    {
+        u32 p = 0;
+        for (int k = 0; k < nmode; ++k) {
+            const int n = t->order[k];
+            const int b = mode_bits(dims[n]);
+            t->fld.pos[n] = p;
+            t->fld.mask[n] = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+            p += b;
+        }
+    }
     altob_status s = build(t, d_cidx, d_vals, vdt, st);
     if (s != ALTOB_OK) {
         altob_destroy(t);
@@ -810,6 +929,8 @@ altob_status altob_destroy(altob_tensor* t)
     cudaDeviceSynchronize();
     dfree(t->d_klo);
     dfree(t->d_khi);
+    dfree(t->d_run_start);
+    dfree(t->d_run_val);
     dfree(t->d_vals);
     for (int n = 0; n < ALTOB_MAX_MODES; ++n) dfree(t->d_oidx[n]);
     dfree(t->scratch);
@@ -840,6 +961,8 @@ altob_status altob_get_info(const altob_tensor* t, altob_info* o)
     o->alto_cr_mask[0] = (u64)t->alto_cr_mask;
     o->alto_cr_mask[1] = (u64)(t->alto_cr_mask >> 64);
     o->device_bytes = t->device_bytes;
+    o->key_bytes = t->d_khi ? 16 : 8;
+    o->nruns = t->nrun;
     return ALTOB_OK;
 }
 
@@ -850,16 +973,25 @@ altob_status altob_dump(const altob_tensor* t, uint64_t* idx, void* vals, uint64
     cudaStream_t st = (cudaStream_t)stream;
     const u64 nnz = t->nnz;
     if (idx && nnz) {
-        std::vector<u64> lo(nnz), hi;
-        ALTOB_CUDA(cudaMemcpyAsync(lo.data(), t->d_klo, nnz * 8, cudaMemcpyDeviceToHost, st));
-        if (t->kw == 2) {
-            hi.resize(nnz);
-            ALTOB_CUDA(cudaMemcpyAsync(hi.data(), t->d_khi, nnz * 8, cudaMemcpyDeviceToHost, st));
+        u64 *olo = nullptr, *ohi = nullptr;
+        ALTOB_TRY(dmalloc_t(&olo, nnz));
+        altob_status s = dmalloc_t(&ohi, nnz);
+        if (s != ALTOB_OK) {
+            dfree(olo);
+            return s;
         }
-        ALTOB_CUDA(cudaStreamSynchronize(st));
+        k_interleave<<<grid_for(nnz, 256), 256, 0, st>>>(t->d_klo, key_src(t), t->alto_bits, nnz, t->dec, t->fld,
+                                                         olo, ohi);
+        std::vector<u64> lo(nnz), hi(nnz);
+        cudaMemcpyAsync(lo.data(), olo, nnz * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(hi.data(), ohi, nnz * 8, cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        dfree(olo);
+        dfree(ohi);
+        if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("dump: ") + cudaGetErrorString(e));
         for (u64 i = 0; i < nnz; ++i) {
             idx[2 * i] = lo[i];
-            idx[2 * i + 1] = t->kw == 2 ? hi[i] : 0;
+            idx[2 * i + 1] = hi[i];
         }
     }
     if (vals && nnz) ALTOB_CUDA(cudaMemcpyAsync(vals, t->d_vals, nnz * val_size(t->vdt), cudaMemcpyDeviceToHost, st));

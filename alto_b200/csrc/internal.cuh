@@ -126,6 +126,55 @@ __host__ __device__ __forceinline__ void split_key(u64 lo, u64 hi, u32 kw[4])
 
 Decoder make_decoder(int nmode, const u128* masks, int alto_bits);
 
+// ------------------------------------------------ device key layout
+//
+// On the device a key keeps the ALTO sort order but stores each mode index
+// as a contiguous bit field (the reference's ALT_PEXT re-encode,
+// alto.hpp:212-244), so reading a mode index is one funnel shift and a mask
+// instead of a bit gather.  Fields are laid out in the ALTO level order
+// (shortest mode first), which puts the longest mode's top bits at the top of
+// the key: those are exactly the most significant ALTO bits, so the key bits
+// above bit 63 are non-decreasing along the sorted stream and can be kept as
+// a short run table instead of a second word per nonzero.  CR bits stay at
+// the reference's positions (alto_bits + k).
+
+struct Fields {
+    int nmode;
+    u32 pos[ALTOB_MAX_MODES];
+    u32 mask[ALTOB_MAX_MODES];
+};
+
+__host__ __device__ __forceinline__ u32 field(u64 lo, u64 hi, u32 pos, u32 mask)
+{
+    u64 v;
+    if (pos >= 64) v = hi >> (pos - 64);
+    else if (pos == 0) v = lo;
+    else v = (lo >> pos) | (hi << (64 - pos));
+    return (u32)v & mask;
+}
+
+// Where the high key word of nonzero i comes from.
+struct KeySrc {
+    const u64* klo;
+    const u64* khi;        // one high word per nonzero, or nullptr
+    const u64* run_start;  // else: sorted run starts of the high word ...
+    const u64* run_val;    // ... and its value on each run
+    int nrun;              // 0: the high word is 0
+};
+
+__device__ __forceinline__ u64 key_hi(const KeySrc& k, u64 i)
+{
+    if (k.khi) return k.khi[i];
+    if (k.nrun == 0) return 0;
+    int lo = 0, hi = k.nrun - 1;  // last run with start <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (k.run_start[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return k.run_val[lo];
+}
+
 // ------------------------------------------------------------- tensor
 
 }  // namespace altob
@@ -140,10 +189,15 @@ struct altob_tensor {
     u128 masks[ALTOB_MAX_MODES] = {0};
     u128 cr_masks[ALTOB_MAX_MODES] = {0};
     u128 alto_mask = 0, alto_cr_mask = 0;
-    altob::Decoder dec;
+    altob::Decoder dec;   // interleaved <-> fields conversion (build / dump)
+    altob::Fields fld;    // device key layout
+    int order[ALTOB_MAX_MODES] = {0};  // ALTO level order of the modes
     // device arrays
     u64* d_klo = nullptr;
-    u64* d_khi = nullptr;
+    u64* d_khi = nullptr;       // explicit high words (or nullptr)
+    u64* d_run_start = nullptr; // implicit high words: run table
+    u64* d_run_val = nullptr;
+    int nrun = 0;
     void* d_vals = nullptr;
     u32* d_oidx[ALTOB_MAX_MODES] = {nullptr};
     // host copies of the small partition tables
@@ -158,6 +212,17 @@ struct altob_tensor {
 namespace altob {
 
 inline size_t val_size(altob_dtype d) { return d == ALTOB_F64 ? 8 : 4; }
+
+inline KeySrc key_src(const altob_tensor* t)
+{
+    KeySrc k;
+    k.klo = t->d_klo;
+    k.khi = t->d_khi;
+    k.run_start = t->d_run_start;
+    k.run_val = t->d_run_val;
+    k.nrun = t->nrun;
+    return k;
+}
 inline u64 fib_reuse(const altob_tensor* t, int n) { return t->nnz / t->dims[n]; }
 
 // Device allocation helpers that record failures as ALTOB_ERR_NOMEM.

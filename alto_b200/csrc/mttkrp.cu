@@ -38,15 +38,19 @@ bool ptr_aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, bool cache, TiledPlan* pl)
 {
     const int V = (int)(16 / fsz);
+    if (R > 128) return fail(ALTOB_ERR_UNSUPPORTED, "rank above 128 in the MTTKRP kernel");
     pl->vec = (aligned && R % V == 0) ? V : 1;
-    pl->lpn = pl->vec == 1 ? 32 : std::max(2, std::min(32, next_pow2((int)((R + pl->vec - 1) / pl->vec))));
-    const u64 per_pass = (u64)pl->lpn * pl->vec;
-    if ((R + per_pass - 1) / per_pass > (u64)MT_CHMAX)
-        return fail(ALTOB_ERR_UNSUPPORTED, "rank too large for the MTTKRP kernel (max " +
-                                               std::to_string(MT_CHMAX * 32 * V) + ")");
+    if (pl->vec == 1) {
+        pl->lpn = 32;
+        pl->ch = 4;
+    } else {
+        const int lanes = (int)((R + pl->vec - 1) / pl->vec);
+        pl->lpn = std::max(2, std::min(32, next_pow2(lanes)));
+        pl->ch = (int)((R + (u64)pl->lpn * pl->vec - 1) / ((u64)pl->lpn * pl->vec));
+    }
     pl->tile = env_int("ALTOB_TILE", 1024);
     pl->tile = std::max(256, (pl->tile / 256) * 256);
-    int cache_bytes = env_int("ALTOB_CACHE_BYTES", 64 * 1024);
+    int cache_bytes = env_int("ALTOB_CACHE_BYTES", 32 * 1024);
     long long rows = (long long)cache_bytes / (long long)(R * fsz);
     pl->hslots = (cache && rows >= 16) ? std::min(floor_pow2(rows), 4096) : 0;
     pl->smem = tiled_smem(t->nmode, pl->tile, pl->hslots, (int)R, fsz);
@@ -63,8 +67,7 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     ALTOB_TRY(plan_tiled(t, R, sizeof(FT), aligned, cache, &pl));
     TiledArgs<FT> a;
     memset(&a, 0, sizeof(a));
-    a.klo = t->d_klo;
-    a.khi = t->d_khi;
+    a.key = key_src(t);
     a.vals = t->d_vals;
     a.perm = perm;
     a.nnz = t->nnz;
@@ -77,11 +80,11 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     a.eps = (FT)eps;
     for (int m = 0; m < t->nmode; ++m) a.U[m] = (const FT*)dU[m];
     a.out = (FT*)dout;
-    a.dec = t->dec;
+    a.fld = t->fld;
     TiledCfg c;
-    c.kw = t->kw;
     c.lpn = pl.lpn;
     c.vec = pl.vec;
+    c.ch = pl.ch;
     c.phi = phi ? 1 : 0;
     c.smem = pl.smem;
     c.grid = dim3(0);
@@ -110,8 +113,7 @@ static altob_status run_atomic_cr(altob_tensor* t, int mode, void* const* dU, u6
     if (!crm) return fail(ALTOB_ERR_ARG, "ATOMIC_CR needs a CR bit for the target mode");
     CrArgsK<FT> a;
     memset(&a, 0, sizeof(a));
-    a.klo = t->d_klo;
-    a.khi = t->d_khi;
+    a.key = key_src(t);
     a.vals = t->d_vals;
     a.nnz = t->nnz;
     a.nprtn = t->nprtn;
@@ -121,13 +123,13 @@ static altob_status run_atomic_cr(altob_tensor* t, int mode, void* const* dU, u6
     a.R = (int)R;
     a.crword = (u64)crm ? 0 : 1;
     a.crbit = (u64)crm ? (u64)crm : (u64)(crm >> 64);
-    if (a.crword == 1 && t->kw != 2) return fail(ALTOB_ERR_ARG, "CR bit outside the stored key");
+
     for (int m = 0; m < t->nmode; ++m) a.U[m] = (const FT*)dU[m];
     a.out = (FT*)dU[mode];
-    a.dec = t->dec;
+    a.fld = t->fld;
     const bool f64 = sizeof(FT) == 8;
-    if (t->vdt == ALTOB_U32) return launch_atomic_cr<FT, u32>(a, t->kw, st);
-    if ((t->vdt == ALTOB_F64) == f64) return launch_atomic_cr<FT, FT>(a, t->kw, st);
+    if (t->vdt == ALTOB_U32) return launch_atomic_cr<FT, u32>(a, st);
+    if ((t->vdt == ALTOB_F64) == f64) return launch_atomic_cr<FT, FT>(a, st);
     return fail(ALTOB_ERR_UNSUPPORTED, "stored value dtype does not match the compute dtype");
 }
 

@@ -7,18 +7,23 @@
 //   mttkrp_alto_atomic_cr     include/alto.hpp:1090-1158  -> k_atomic_cr
 //   CalculatePhi_alto_*       include/apr.hpp:383-848     -> k_tiled<..., PHI=true>
 //
-// k_tiled: a persistent CTA walks tiles of TILE consecutive nonzeros of the
-// ALTO-ordered stream.  Phase A (one thread per nonzero) loads the key and
-// value with coalesced loads, decodes every mode index with the compress
-// network and claims a shared-memory accumulator row for the output index
-// (direct-mapped on its low bits).  Phase B (a group of LPN lanes per
-// nonzero, VEC elements per lane, 16-byte loads) gathers the factor rows,
-// forms val * Khatri-Rao row (or the Phi row) and adds it to the claimed
-// shared-memory row, or straight to global memory when the slot belongs to
-// another index.  Phase C flushes every claimed row once with vector
-// atomics.  This is the GPU form of the reference's per-partition temporary
-// rows plus pull reduction: the tile is the partition and the flush is the
-// pull.
+// k_tiled: a persistent CTA walks tiles of `tile` consecutive nonzeros of
+// the ALTO-ordered stream (the GPU analogue of the reference's line
+// segments).
+//   Phase A, one thread per nonzero: coalesced loads of key and value, mode
+//     indices read as bit fields, and a shared-memory accumulator row claimed
+//     for the output index (direct-mapped on its low bits; claims are
+//     appended to a list with one atomic per warp).
+//   Phase B, LPN lanes per nonzero with VEC elements each (16-byte loads):
+//     gather the other modes' factor rows, form val * (Khatri-Rao row) (or
+//     the Phi row), add into the claimed row; a nonzero whose slot belongs to
+//     another index goes straight to global memory with a vector atomic.
+//     Lane group q adds its VEC elements in the order rotated by q, so the
+//     NPW groups of a warp hit disjoint shared-memory banks.
+//   Phase C: every claimed row is flushed once with vector atomics and
+//     cleared.
+// The tile is the segment and the flush is the pull of the reference's
+// da_mem_pull; only rows touched by several tiles meet in global memory.
 #pragma once
 
 #include "internal.cuh"
@@ -27,7 +32,6 @@ namespace altob {
 
 constexpr int MT_THREADS = 256;
 constexpr int MT_WARPS = MT_THREADS / 32;
-constexpr int MT_CHMAX = 4;  // rank chunks kept in registers
 
 template <typename FT, int VEC>
 struct VecT;
@@ -83,10 +87,59 @@ __device__ __forceinline__ void gred(FT* p, const FT* x)
     }
 }
 
+// y[e] = x[(e + r) % VEC] with r fixed per lane (branch-free selects).
+template <typename FT, int VEC>
+__device__ __forceinline__ void rotate(const FT* x, int r, FT* y)
+{
+    if constexpr (VEC == 1) {
+        y[0] = x[0];
+    } else if constexpr (VEC == 2) {
+        const bool s = r & 1;
+        y[0] = s ? x[1] : x[0];
+        y[1] = s ? x[0] : x[1];
+    } else {
+        FT t[4];
+        const bool s1 = r & 1, s2 = r & 2;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) t[e] = s1 ? x[(e + 1) & 3] : x[e];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) y[e] = s2 ? t[(e + 2) & 3] : t[e];
+    }
+}
+
+// x[e] *= y[e]; FP32 pairs use the packed FP32x2 multiply of sm_100 (same
+// IEEE round-to-nearest result as two scalar multiplies).
+template <typename FT, int VEC>
+__device__ __forceinline__ void vmul(FT* x, const FT* y)
+{
+    if constexpr (sizeof(FT) == 4 && VEC % 2 == 0) {
+#pragma unroll
+        for (int e = 0; e < VEC; e += 2) {
+            const float2 r = __fmul2_rn(make_float2(x[e], x[e + 1]), make_float2(y[e], y[e + 1]));
+            x[e] = r.x;
+            x[e + 1] = r.y;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) x[e] *= y[e];
+    }
+}
+
+// Index of the high-word run that contains nonzero g (uniform per tile).
+__device__ __forceinline__ int run_of(const KeySrc& k, u64 g)
+{
+    int lo = 0, hi = k.nrun - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (k.run_start[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename FT>
 struct TiledArgs {
-    const u64* klo;
-    const u64* khi;
+    KeySrc key;
     const void* vals;
     const u32* perm;  // read order (oidx) or nullptr for ALTO order
     u64 nnz;
@@ -99,7 +152,7 @@ struct TiledArgs {
     FT eps;      // Phi: eps_div_zero
     const FT* U[ALTOB_MAX_MODES];
     FT* out;
-    Decoder dec;
+    Fields fld;
 };
 
 // Dynamic shared-memory bytes of k_tiled.
@@ -114,11 +167,16 @@ inline size_t tiled_smem(int nmode, int tile, int hslots, int R, size_t fsz)
     return b;
 }
 
-template <typename FT, typename VT, int KW, int LPN, int VEC, bool PHI>
+// NM: number of modes (0 = any, read from the arguments).  R <= LPN*VEC*CH.
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 {
+    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    constexpr int NPW = 32 / LPN;
+    constexpr int UNR = 2;  // warp steps issued together in phase B
     extern __shared__ __align__(16) unsigned char smem[];
-    const int tile = a.tile, nmode = a.nmode, R = a.R, H = a.hslots;
+    const int tile = a.tile, R = a.R, H = a.hslots;
+    const int nmode = NM ? NM : a.nmode;
     u32* crd = reinterpret_cast<u32*>(smem);
     int* slot = reinterpret_cast<int*>(crd + (size_t)nmode * tile);
     FT* val = reinterpret_cast<FT*>(slot + tile);
@@ -139,125 +197,197 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 
     const VT* vals = reinterpret_cast<const VT*>(a.vals);
     const int target = a.target;
-    constexpr int NPW = 32 / LPN;
     const int sub = lane % LPN, q = lane / LPN;
+    const int rot = q % VEC;
     const int per_warp = tile / MT_WARPS;
-    const int nch = (R + LPN * VEC - 1) / (LPN * VEC);
+    const u32 lt_mask = (1u << lane) - 1u;
+    // the other modes' factor matrices and index rows (static register indices)
+    const FT* Uo[MM - 1];
+    int oo[MM - 1];
+#pragma unroll
+    for (int k = 0; k < MM - 1; ++k) {
+        const int m = k < target ? k : k + 1;
+        Uo[k] = a.U[k < target ? k : (k + 1 < MM ? k + 1 : k)];
+        oo[k] = m * tile;
+    }
+    const int nother = nmode - 1;
 
     for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) {
-        // ---- phase A: load, decode, claim accumulator rows
+        // ---- phase A: load, read mode indices, claim accumulator rows
         const u64 g0 = ti * (u64)tile;
+        // high key word: one compare per nonzero unless the tile spans
+        // several runs (or reads through a permutation)
+        u64 hcur = 0, hnext = 0, nstart = ~0ull;
+        bool slow_hi = a.perm != nullptr;
+        if (!a.key.khi && a.key.nrun && !slow_hi) {
+            const int r = run_of(a.key, g0);
+            hcur = a.key.run_val[r];
+            if (r + 1 < a.key.nrun) {
+                nstart = a.key.run_start[r + 1];
+                hnext = a.key.run_val[r + 1];
+                if (r + 2 < a.key.nrun && a.key.run_start[r + 2] < g0 + (u64)tile) slow_hi = true;
+            }
+        }
         for (int it = tid; it < tile; it += MT_THREADS) {
             const u64 g = g0 + it;
             int sl = -2;
+            bool claimed = false;
+            u32 h = 0;
             if (g < a.nnz) {
                 const u64 pos = a.perm ? (u64)a.perm[g] : g;
-                u32 w[4];
-                split_key(a.klo[pos], KW == 2 ? a.khi[pos] : 0ull, w);
-                val[it] = (FT)vals[pos];
+                const u64 lo = a.key.klo[pos];
+                const VT vv = vals[pos];
+                u64 hi;
+                if (a.key.khi) hi = a.key.khi[pos];
+                else if (a.key.nrun == 0) hi = 0;
+                else if (slow_hi) hi = key_hi(a.key, pos);
+                else hi = g >= nstart ? hnext : hcur;
+                val[it] = (FT)vv;
                 u32 trow = 0;
-                for (int m = 0; m < nmode; ++m) {
-                    u32 c = decode_mode(w, a.dec.md[m], a.dec.nwords);
+#pragma unroll
+                for (int m = 0; m < MM; ++m) {
+                    if (NM == 0 && m >= nmode) break;
+                    const u32 c = field(lo, hi, a.fld.pos[m], a.fld.mask[m]);
                     crd[(size_t)m * tile + it] = c;
                     if (m == target) trow = c;
                 }
                 sl = -1;
                 if (H) {
-                    u32 h = trow & (u32)(H - 1);
-                    u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
+                    h = trow & (u32)(H - 1);
+                    const u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
                     if (old == 0u) {
-                        used[atomicAdd(&nused, 1u)] = h;
+                        claimed = true;
                         sl = (int)h;
                     } else if (old == trow + 1u) {
                         sl = (int)h;
                     }
                 }
-            }
-            else {
+            } else {
                 // tail of the last tile: harmless index 0, value 0, no writes
-                for (int m = 0; m < nmode; ++m) crd[(size_t)m * tile + it] = 0u;
+#pragma unroll
+                for (int m = 0; m < MM; ++m) {
+                    if (NM == 0 && m >= nmode) break;
+                    crd[(size_t)m * tile + it] = 0u;
+                }
                 val[it] = FT(0);
             }
             slot[it] = sl;
-        }
-        __syncthreads();
-
-        // ---- phase B: gather factor rows, accumulate
-        for (int j = warp * per_warp; j < (warp + 1) * per_warp; j += NPW) {
-            const int it = j + q;
-            const int sl = slot[it];  // -2: no nonzero (kept in the loop for the Phi shuffles)
-            const FT v = val[it];
-            FT x[MT_CHMAX][VEC];
-#pragma unroll
-            for (int ch = 0; ch < MT_CHMAX; ++ch)
-#pragma unroll
-                for (int e = 0; e < VEC; ++e) x[ch][e] = PHI ? FT(1) : v;
-            for (int m = 0; m < nmode; ++m) {
-                if (m == target) continue;
-                const FT* row = a.U[m] + (size_t)crd[(size_t)m * tile + it] * R;
-#pragma unroll
-                for (int ch = 0; ch < MT_CHMAX; ++ch) {
-                    const int r0 = ch * LPN * VEC + sub * VEC;
-                    if (ch < nch && r0 < R) {
-                        FT y[VEC];
-                        vload<FT, VEC>(row + r0, y);
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) x[ch][e] *= y[e];
-                    }
-                }
-            }
-            const u32 trow = crd[(size_t)target * tile + it];
-            if constexpr (PHI) {
-                // v / max(<B[trow,:], krp>, eps), apr.hpp:452-462
-                const FT* brow = a.U[target] + (size_t)trow * R;
-                FT dot = FT(0);
-#pragma unroll
-                for (int ch = 0; ch < MT_CHMAX; ++ch) {
-                    const int r0 = ch * LPN * VEC + sub * VEC;
-                    if (ch < nch && r0 < R) {
-                        FT y[VEC];
-                        vload<FT, VEC>(brow + r0, y);
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) dot += y[e] * x[ch][e];
-                    }
-                }
-#pragma unroll
-                for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o, LPN);
-                const FT s = v / (dot > a.eps ? dot : a.eps);
-#pragma unroll
-                for (int ch = 0; ch < MT_CHMAX; ++ch)
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) x[ch][e] *= s;
-            }
-#pragma unroll
-            for (int ch = 0; ch < MT_CHMAX; ++ch) {
-                const int r0 = ch * LPN * VEC + sub * VEC;
-                if (ch < nch && r0 < R && sl != -2) {
-                    if (sl >= 0) {
-                        FT* dst = acc + (size_t)sl * R + r0;
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) atomicAdd(dst + e, x[ch][e]);
-                    } else {
-                        gred<FT, VEC>(a.out + (size_t)trow * R + r0, x[ch]);
-                    }
-                }
+            // append this warp's claims to the list with one atomic
+            const u32 cm = __ballot_sync(0xffffffffu, claimed);
+            if (cm) {
+                u32 base = 0;
+                if (lane == 0) base = atomicAdd(&nused, (u32)__popc(cm));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (claimed) used[base + __popc(cm & lt_mask)] = h;
             }
         }
         __syncthreads();
 
-        // ---- phase C: flush claimed rows
+        // ---- phase B: gather factor rows (UNR steps in flight), accumulate
+        for (int j = warp * per_warp; j < (warp + 1) * per_warp; j += NPW * UNR) {
+            int its[UNR], sls[UNR];
+            FT vs[UNR];
+            FT x[UNR][CH][VEC];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                its[u] = j + u * NPW + q;
+                sls[u] = slot[its[u]];  // -2: no nonzero (kept for the Phi shuffles)
+                vs[u] = val[its[u]];
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) x[u][ch][e] = PHI ? FT(1) : vs[u];
+            }
+            FT y[UNR][MM - 1][CH][VEC];
+#pragma unroll
+            for (int k = 0; k < MM - 1; ++k) {
+                if (NM == 0 && k >= nother) break;
+#pragma unroll
+                for (int u = 0; u < UNR; ++u) {
+                    const FT* row = Uo[k] + (size_t)crd[oo[k] + its[u]] * R;
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch) {
+                        const int r0 = ch * LPN * VEC + sub * VEC;
+                        if (r0 < R) vload<FT, VEC>(row + r0, y[u][k][ch]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < MM - 1; ++k) {
+                if (NM == 0 && k >= nother) break;
+#pragma unroll
+                for (int u = 0; u < UNR; ++u)
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch) {
+                        const int r0 = ch * LPN * VEC + sub * VEC;
+                        if (r0 < R) vmul<FT, VEC>(x[u][ch], y[u][k][ch]);
+                    }
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const u32 trow = crd[(size_t)target * tile + its[u]];
+                if constexpr (PHI) {
+                    // v / max(<B[trow,:], krp>, eps), apr.hpp:452-462
+                    const FT* brow = a.U[target] + (size_t)trow * R;
+                    FT dot = FT(0);
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch) {
+                        const int r0 = ch * LPN * VEC + sub * VEC;
+                        if (r0 < R) {
+                            FT b[VEC];
+                            vload<FT, VEC>(brow + r0, b);
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) dot += b[e] * x[u][ch][e];
+                        }
+                    }
+#pragma unroll
+                    for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o, LPN);
+                    const FT sc = vs[u] / (dot > a.eps ? dot : a.eps);
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) x[u][ch][e] *= sc;
+                }
+                const int sl = sls[u];
+                if (sl == -2) continue;
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch) {
+                    const int r0 = ch * LPN * VEC + sub * VEC;
+                    if (r0 < R) {
+                        if (sl >= 0) {
+                            FT z[VEC];
+                            rotate<FT, VEC>(x[u][ch], rot, z);
+                            FT* dst = acc + (size_t)sl * R + r0;
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) atomicAdd(dst + ((e + rot) % VEC), z[e]);
+                        } else {
+                            gred<FT, VEC>(a.out + (size_t)trow * R + r0, x[u][ch]);
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- phase C: flush claimed rows (NPW rows per warp step)
         if (H) {
             const u32 nu = nused;
-            for (u32 k = warp; k < nu; k += MT_WARPS) {
-                const u32 h = used[k];
-                const u32 row = tag[h] - 1u;
-                FT* src = acc + (size_t)h * R;
-                FT* dst = a.out + (size_t)row * R;
-                for (int r = lane * VEC; r < R; r += 32 * VEC) {
-                    FT y[VEC];
-                    vload_plain<FT, VEC>(src + r, y);
-                    gred<FT, VEC>(dst + r, y);
-                    vstore_zero<FT, VEC>(src + r);
+            for (u32 k = (u32)warp * NPW; k < nu; k += MT_WARPS * NPW) {
+                const u32 kk = k + q;
+                if (kk < nu) {
+                    const u32 hh = used[kk];
+                    FT* src = acc + (size_t)hh * R;
+                    FT* dst = a.out + (size_t)(tag[hh] - 1u) * R;
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch) {
+                        const int r0 = ch * LPN * VEC + sub * VEC;
+                        if (r0 < R) {
+                            FT z[VEC];
+                            vload_plain<FT, VEC>(src + r0, z);
+                            gred<FT, VEC>(dst + r0, z);
+                            vstore_zero<FT, VEC>(src + r0);
+                        }
+                    }
                 }
             }
             __syncthreads();
@@ -271,8 +401,7 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 
 template <typename FT>
 struct CrArgsK {
-    const u64* klo;
-    const u64* khi;
+    KeySrc key;
     const void* vals;
     u64 nnz;
     u64 per;  // nonzeros per reference partition
@@ -284,14 +413,14 @@ struct CrArgsK {
     u64 crbit;   // bit mask inside that word
     const FT* U[ALTOB_MAX_MODES];
     FT* out;
-    Decoder dec;
+    Fields fld;
 };
 
 // mttkrp_alto_atomic_cr (alto.hpp:1090-1158): one warp owns one reference
 // partition and walks it in order, so rows owned by that partition (CR bit
 // clear) are updated with plain read-modify-write and shared rows (CR bit
 // set) with atomics.
-template <typename FT, typename VT, int KW>
+template <typename FT, typename VT>
 __global__ void __launch_bounds__(MT_THREADS) k_atomic_cr(CrArgsK<FT> a)
 {
     const int lane = threadIdx.x & 31;
@@ -303,13 +432,11 @@ __global__ void __launch_bounds__(MT_THREADS) k_atomic_cr(CrArgsK<FT> a)
         if (s > a.nnz) s = a.nnz;
         if (e > a.nnz) e = a.nnz;
         for (u64 i = s; i < e; ++i) {
-            u64 lo = a.klo[i], hi = KW == 2 ? a.khi[i] : 0ull;
-            u32 w[4];
-            split_key(lo, hi, w);
+            const u64 lo = a.key.klo[i], hi = key_hi(a.key, i);
             const bool shared = ((a.crword ? hi : lo) & a.crbit) != 0;
             const FT v = (FT)vals[i];
             u32 c[ALTOB_MAX_MODES];
-            for (int m = 0; m < a.nmode; ++m) c[m] = decode_mode(w, a.dec.md[m], a.dec.nwords);
+            for (int m = 0; m < a.nmode; ++m) c[m] = field(lo, hi, a.fld.pos[m], a.fld.mask[m]);
             for (int r = lane; r < a.R; r += 32) {
                 FT x = v;
                 for (int m = 0; m < a.nmode; ++m)

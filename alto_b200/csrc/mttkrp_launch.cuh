@@ -8,7 +8,7 @@
 namespace altob {
 
 struct TiledCfg {
-    int kw, lpn, vec, phi;
+    int lpn, vec, ch, phi;
     dim3 grid;
     size_t smem;
 };
@@ -17,14 +17,14 @@ template <typename FT, typename VT>
 altob_status launch_tiled(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* max_blocks_per_sm);
 
 template <typename FT, typename VT>
-altob_status launch_atomic_cr(const CrArgsK<FT>& a, int kw, cudaStream_t st);
+altob_status launch_atomic_cr(const CrArgsK<FT>& a, cudaStream_t st);
 
-// Resolves the kernel for (KW, LPN, VEC, PHI), sets its shared-memory limit
-// once, and launches it (or only reports occupancy when grid.x == 0).
-template <typename FT, typename VT, int KW, int LPN, int VEC, bool PHI>
+// Sets the kernel's shared-memory limit once and launches it (or only
+// reports occupancy when grid.x == 0).
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
 {
-    auto k = k_tiled<FT, VT, KW, LPN, VEC, PHI>;
+    auto k = k_tiled<FT, VT, NM, LPN, VEC, CH, PHI>;
     static size_t configured = 0;
     if (c.smem > configured) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
@@ -43,17 +43,19 @@ altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t 
     return ALTOB_OK;
 }
 
-template <typename FT, typename VT, int KW, bool PHI>
-altob_status launch_lpn(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+// (lanes per nonzero, elements per lane, chunks) -> kernel
+template <typename FT, typename VT, int NM, bool PHI>
+altob_status launch_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     constexpr int V = 16 / sizeof(FT);
-    if (c.vec == 1) return launch_one<FT, VT, KW, 32, 1, PHI>(a, c, st, bps);
+    if (c.vec == 1) return launch_one<FT, VT, NM, 32, 1, 4, PHI>(a, c, st, bps);
+    if (c.ch == 2) return launch_one<FT, VT, NM, 32, V, 2, PHI>(a, c, st, bps);
     switch (c.lpn) {
-    case 2: return launch_one<FT, VT, KW, 2, V, PHI>(a, c, st, bps);
-    case 4: return launch_one<FT, VT, KW, 4, V, PHI>(a, c, st, bps);
-    case 8: return launch_one<FT, VT, KW, 8, V, PHI>(a, c, st, bps);
-    case 16: return launch_one<FT, VT, KW, 16, V, PHI>(a, c, st, bps);
-    case 32: return launch_one<FT, VT, KW, 32, V, PHI>(a, c, st, bps);
+    case 2: return launch_one<FT, VT, NM, 2, V, 1, PHI>(a, c, st, bps);
+    case 4: return launch_one<FT, VT, NM, 4, V, 1, PHI>(a, c, st, bps);
+    case 8: return launch_one<FT, VT, NM, 8, V, 1, PHI>(a, c, st, bps);
+    case 16: return launch_one<FT, VT, NM, 16, V, 1, PHI>(a, c, st, bps);
+    case 32: return launch_one<FT, VT, NM, 32, V, 1, PHI>(a, c, st, bps);
     }
     return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
 }
@@ -63,19 +65,17 @@ altob_status launch_lpn(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t 
     altob_status launch_tiled<FT, VT>(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st,      \
                                       int* bps)                                                        \
     {                                                                                                  \
-        if (c.kw == 2)                                                                                 \
-            return c.phi ? launch_lpn<FT, VT, 2, true>(a, c, st, bps)                                  \
-                         : launch_lpn<FT, VT, 2, false>(a, c, st, bps);                                \
-        return c.phi ? launch_lpn<FT, VT, 1, true>(a, c, st, bps) : launch_lpn<FT, VT, 1, false>(a, c, st, bps); \
+        if (a.nmode == 3)                                                                              \
+            return c.phi ? launch_shape<FT, VT, 3, true>(a, c, st, bps)                                \
+                         : launch_shape<FT, VT, 3, false>(a, c, st, bps);                              \
+        return c.phi ? launch_shape<FT, VT, 0, true>(a, c, st, bps) : launch_shape<FT, VT, 0, false>(a, c, st, bps); \
     }                                                                                                  \
     template <>                                                                                        \
-    altob_status launch_atomic_cr<FT, VT>(const CrArgsK<FT>& a, int kw, cudaStream_t st)               \
+    altob_status launch_atomic_cr<FT, VT>(const CrArgsK<FT>& a, cudaStream_t st)                       \
     {                                                                                                  \
-        int warps = a.nprtn;                                                                           \
-        int blocks = (warps * 32 + MT_THREADS - 1) / MT_THREADS;                                        \
+        int blocks = (a.nprtn * 32 + MT_THREADS - 1) / MT_THREADS;                                      \
         if (blocks < 1) blocks = 1;                                                                    \
-        if (kw == 2) k_atomic_cr<FT, VT, 2><<<blocks, MT_THREADS, 0, st>>>(a);                          \
-        else k_atomic_cr<FT, VT, 1><<<blocks, MT_THREADS, 0, st>>>(a);                                  \
+        k_atomic_cr<FT, VT><<<blocks, MT_THREADS, 0, st>>>(a);                                          \
         cudaError_t e = cudaGetLastError();                                                            \
         if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("k_atomic_cr: ") + cudaGetErrorString(e)); \
         return ALTOB_OK;                                                                               \

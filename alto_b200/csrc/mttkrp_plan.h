@@ -6,7 +6,7 @@
 namespace altob {
 
 struct TiledPlan {
-    int vec, lpn, tile, hslots;
+    int vec, lpn, ch, tile, hslots;
     size_t smem;
 };
 

@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--draws", type=int, default=DRAWS, help="Zipf draws per mode (smaller = profiling case)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--cpu-sample-draws", type=int, default=20_000_000)
+    p.add_argument("--cpu-sample-draws", type=int, default=40_000_000)
     p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
     p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
     return p.parse_args()
@@ -341,8 +341,7 @@ def run_altob(args):
     value = ws * nnz * 3 / (ms_step / 1e3) / 1e9
 
     # roofline of the MTTKRP kernel: algorithmic bytes per launch
-    kw_bytes = 16 if info["lit_bits"] == 128 else 8
-    stream_b = nnz * (kw_bytes + 4)
+    stream_b = nnz * (info["key_bytes"] + 4)  # index words as stored on the device + FP32 value
     fac_b = [d * RANK * 4 for d in DIMS]
     launch_ms = [[], [], []]
     for k in range(args.steps):

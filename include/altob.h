@@ -76,6 +76,8 @@ typedef struct {
     uint64_t alto_mask[2];
     uint64_t alto_cr_mask[2];
     uint64_t device_bytes; /* HBM held by the handle */
+    uint64_t key_bytes;    /* bytes of index stored per nonzero on the device */
+    int nruns;             /* high index words kept as a run table (0: none) */
 } altob_info;
 
 /* COO tensor in host memory (SparseTensor, sptensor.hpp:8-25): cidx is
