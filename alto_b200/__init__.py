@@ -75,6 +75,7 @@ SIGNATURES = {
     "altob_cp_apr": (_i, [_vp, _i, _vp, _vp, _u64, _i, _i, _d, _d, _d, _d, _i, _dp, _vp]),
     "altob_phi": (_i, [_vp, _i, _i, _vp, _u64, _d, _vp, _vp]),
     "altob_loglik": (_i, [_vp, _i, _vp, _vp, _u64, _d, _dp, _vp]),
+    "altob_loglik_noalloc": (_i, [_vp, _i, _vp, _vp, _u64, _d, _dp, _vp]),
     "altob_read_tns": (_i, [C.c_char_p, _i, C.POINTER(C.POINTER(_Coo))]),
     "altob_read_bin": (_i, [C.c_char_p, C.POINTER(C.POINTER(_Coo))]),
     "altob_write_bin": (_i, [C.c_char_p, C.POINTER(_Coo)]),

@@ -9,6 +9,8 @@
 // KKT violation and the log-likelihood accumulate in FP64.
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "dense.cuh"
@@ -323,3 +325,74 @@ altob_status altob_loglik(altob_tensor* t, altob_dtype ftype, void* const* d_fac
 
 }  // extern "C"
 
+
+// ---------------------------------------------------------------------------
+// altob_loglik_noalloc: the log-likelihood for callers that cannot allocate
+// device memory.  Some callers own every byte of device memory through their
+// own pool or arena, run where the CUDA allocator must not be entered, or
+// need a call whose memory footprint is fixed before it runs; altob_loglik
+// takes its scratch from the tensor handle's cache, which may call
+// cudaMalloc.  This variant keeps its scratch in the file-scope array below
+// instead.  The caller still passes the tensor, factors and lambda.
+
+namespace altob {
+
+// Largest rank the fixed scratch holds (the library's model rank limit):
+// lambda and column sums (2R doubles) plus the two accumulators;
+// 2 * 112 + 8 doubles = 1856 bytes per device.
+constexpr int LOGLIK_NOALLOC_MAX_RANK = 112;
+static __device__ __align__(256) double g_loglik_scratch[2 * LOGLIK_NOALLOC_MAX_RANK + 8];
+
+// Device address of g_loglik_scratch on the current device.  Host code may
+// not use the array's name as a device pointer, so the address is looked up
+// once per device (on the first call there) and cached.
+static altob_status loglik_scratch_address(double** out)
+{
+    static std::mutex mu;
+    static std::vector<double*> addr;
+    int dev = 0;
+    ALTOB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((size_t)dev >= addr.size()) addr.resize((size_t)dev + 1, nullptr);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_loglik_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(ALTOB_ERR_CUDA, std::string("cudaGetSymbolAddress(g_loglik_scratch): ") + cudaGetErrorString(e));
+        addr[dev] = (double*)p;
+    }
+    *out = addr[dev];
+    return ALTOB_OK;
+}
+
+}  // namespace altob
+
+extern "C" altob_status altob_loglik_noalloc(altob_tensor* t, altob_dtype ftype, void* const* d_factors,
+                                             void* d_lambda, uint64_t rank, double eps_div_zero, double* loglik,
+                                             void* stream)
+{
+    if (rank > (uint64_t)LOGLIK_NOALLOC_MAX_RANK)
+        return fail(ALTOB_ERR_ARG, "altob_loglik_noalloc: rank " + std::to_string(rank) +
+                                       " exceeds the fixed scratch (maximum rank " +
+                                       std::to_string(LOGLIK_NOALLOC_MAX_RANK) + ")");
+    ALTOB_TRY(check_model(t, ftype, d_factors, rank));
+    if (!d_lambda || !loglik) return fail(ALTOB_ERR_ARG, "NULL argument");
+    double* d = nullptr;
+    ALTOB_TRY(loglik_scratch_address(&d));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int R = (int)rank;
+    // every scratch word is written before it is read in this call:
+    // lambda is loaded from d_lambda, the others are zeroed by their kernels
+    double *lam = d, *colacc = d + R, *ll = d + 2 * R, *fsum = d + 2 * R + 1;
+    if (ftype == ALTOB_F64) {
+        ALTOB_TRY(vec_from<double>(lam, (const double*)d_lambda, R, st));
+        ALTOB_TRY(loglik_impl<double>(t, (double**)d_factors, lam, colacc, ll, fsum, R, eps_div_zero, loglik, st));
+        ALTOB_TRY(vec_to<double>((double*)d_lambda, lam, R, st));
+    } else {
+        ALTOB_TRY(vec_from<float>(lam, (const float*)d_lambda, R, st));
+        ALTOB_TRY(loglik_impl<float>(t, (float**)d_factors, lam, colacc, ll, fsum, R, eps_div_zero, loglik, st));
+        ALTOB_TRY(vec_to<float>((float*)d_lambda, lam, R, st));
+    }
+    ALTOB_CUDA(cudaStreamSynchronize(st));
+    return ALTOB_OK;
+}

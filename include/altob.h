@@ -206,6 +206,25 @@ ALTOB_API altob_status altob_loglik(altob_tensor* t, altob_dtype ftype,
                           uint64_t rank, double eps_div_zero,
                           double* loglik, void* stream);
 
+/* No counterpart in the reference.  altob_loglik without device allocation,
+ * for callers that cannot call cudaMalloc: code that owns all device memory
+ * through its own pool or arena, code running where the CUDA allocator must
+ * not be entered, or callers that need a fixed memory footprint.  The caller
+ * passes the same tensor, factors and lambda as to altob_loglik and gets the
+ * same result.  The scratch (lambda, column sums, two accumulators) is a
+ * fixed device array inside the library: rank at most 112 (1856 bytes, held
+ * on every GPU that loads the library until the process exits); a larger
+ * rank returns ALTOB_ERR_ARG.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller.  Synchronous on `stream`. */
+ALTOB_API altob_status altob_loglik_noalloc(altob_tensor* t, altob_dtype ftype,
+                                            void* const* d_factors,
+                                            void* d_lambda, uint64_t rank,
+                                            double eps_div_zero,
+                                            double* loglik, void* stream);
+
 /* ---- tensor files ------------------------------------------------------
  * Replaces ImportSparseTensor (sptensor.cpp:165-258).  The .tns reader
  * follows the reference (dims = largest index seen, '#' comments and empty
