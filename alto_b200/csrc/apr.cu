@@ -292,6 +292,7 @@ altob_status altob_cp_apr(altob_tensor* t, altob_dtype ftype, void* const* d_fac
     if (max_iters < 1 || max_inner < 1) return fail(ALTOB_ERR_ARG, "iteration counts must be >= 1");
     if (t->nnz == 0) return fail(ALTOB_ERR_ARG, "CP-APR on an empty tensor");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     if (ftype == ALTOB_F64)
         return cp_apr_impl<double>(t, (double**)d_factors, (double*)d_lambda, (int)rank, max_iters, max_inner,
                                    epsilon, eps_div_zero, kappa_tol, kappa, dobench, summary, st);
@@ -305,6 +306,7 @@ altob_status altob_loglik(altob_tensor* t, altob_dtype ftype, void* const* d_fac
     ALTOB_TRY(check_model(t, ftype, d_factors, rank));
     if (!d_lambda || !loglik) return fail(ALTOB_ERR_ARG, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const int R = (int)rank;
     void* base = nullptr;
     ALTOB_TRY(tensor_scratch(t, (4 * (size_t)R + 8) * sizeof(double), &base));

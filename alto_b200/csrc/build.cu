@@ -28,10 +28,15 @@ altob_status fail(altob_status s, const std::string& msg)
     return s;
 }
 
+static thread_local cudaStream_t g_alloc_stream = 0;
+
+StreamScope::StreamScope(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+StreamScope::~StreamScope() { g_alloc_stream = prev; }
+
 altob_status dmalloc(void** p, size_t bytes)
 {
     *p = nullptr;
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 1);
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 1, g_alloc_stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
@@ -43,15 +48,14 @@ altob_status dmalloc(void** p, size_t bytes)
 
 void dfree(void* p)
 {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, g_alloc_stream);
 }
 
 altob_status tensor_scratch(altob_tensor* t, size_t bytes, void** out)
 {
     if (bytes > t->scratch_bytes) {
         if (t->scratch) {
-            cudaDeviceSynchronize();
-            dfree(t->scratch);
+            dfree(t->scratch);  // stream-ordered: after this stream's earlier uses
             t->scratch = nullptr;
             t->scratch_bytes = 0;
         }
@@ -764,13 +768,14 @@ static altob_status build(altob_tensor* t, const u64* d_cidx, const void* d_vals
         e = cudaStreamSynchronize(st);
         if (e == cudaSuccess && hc[1] == 0 && hc[0] <= cap) {
             std::vector<u64> hs(hc[0]);
-            cudaMemcpy(hs.data(), starts, hc[0] * sizeof(u64), cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(hs.data(), starts, hc[0] * sizeof(u64), cudaMemcpyDeviceToHost, st);
+            cudaStreamSynchronize(st);
             std::sort(hs.begin(), hs.end());
             u64 *rs = nullptr, *rv = nullptr;
             s = dmalloc_t(&rs, hc[0]);
             if (s == ALTOB_OK) s = dmalloc_t(&rv, hc[0]);
             if (s == ALTOB_OK) {
-                cudaMemcpy(rs, hs.data(), hc[0] * sizeof(u64), cudaMemcpyHostToDevice);
+                cudaMemcpyAsync(rs, hs.data(), hc[0] * sizeof(u64), cudaMemcpyHostToDevice, st);
                 k_gather_u64<<<std::max(1u, (hc[0] + 255) / 256), 256, 0, st>>>(khi, rs, hc[0], rv);
                 e = cudaStreamSynchronize(st);
                 if (e == cudaSuccess) {
@@ -894,6 +899,7 @@ altob_status altob_create(int nmode, const uint64_t* dims, uint64_t nnz, const u
     if (!dims) return fail(ALTOB_ERR_ARG, "dims is NULL");
     if (nmode < 1 || nmode > ALTOB_MAX_MODES) return fail(ALTOB_ERR_ARG, "nmode must be 1..5");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     u64* d_cidx = nullptr;
     void* d_vals = nullptr;
     size_t vsz = val_size(val_dtype);
@@ -920,13 +926,17 @@ altob_status altob_create_device(int nmode, const uint64_t* dims, uint64_t nnz, 
                                  altob_tensor** out)
 {
     if (!dims) return fail(ALTOB_ERR_ARG, "dims is NULL");
+    StreamScope scope((cudaStream_t)stream);
     return create_common(nmode, dims, nnz, d_cidx, d_vals, val_dtype, nprtn, lit_bits, (cudaStream_t)stream, out);
 }
 
 altob_status altob_destroy(altob_tensor* t)
 {
     if (!t) return ALTOB_OK;
-    cudaDeviceSynchronize();
+    // frees are ordered on the legacy default stream, i.e. after the work
+    // already issued on blocking streams; work on non-blocking streams that
+    // uses the tensor must be finished by the caller first
+    StreamScope scope(0);
     dfree(t->d_klo);
     dfree(t->d_khi);
     dfree(t->d_run_start);
@@ -971,6 +981,7 @@ altob_status altob_dump(const altob_tensor* t, uint64_t* idx, void* vals, uint64
 {
     if (!t) return fail(ALTOB_ERR_ARG, "NULL tensor");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const u64 nnz = t->nnz;
     if (idx && nnz) {
         u64 *olo = nullptr, *ohi = nullptr;

@@ -117,6 +117,7 @@ extern "C" altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype, void* 
     if (t->nmode < 2) return fail(ALTOB_ERR_ARG, "CP-ALS needs at least two modes");
     if (t->nnz == 0) return fail(ALTOB_ERR_ARG, "CP-ALS on an empty tensor (the fit divides by its norm)");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     if (ftype == ALTOB_F64)
         return cpd_als_impl<double>(t, (double**)d_factors, (double*)d_lambda, (int)rank, max_iters, epsilon, fits,
                                     iters, st);

@@ -1,6 +1,7 @@
 // dense.cu -- dense kernels for the CP-ALS / CP-APR updates (see dense.cuh).
 // Every reduction accumulates in FP64; factor storage is FT (float/double).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 #include "dense.cuh"
@@ -281,10 +282,12 @@ altob_status solve_setup(const double* G, int nmode, int target, int R, double* 
 {
     if (R > SOLVE_MAX_RANK) return fail(ALTOB_ERR_UNSUPPORTED, "rank above 112 in the R x R solve");
     size_t smem = (size_t)2 * R * R * sizeof(double);
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
+    static std::atomic<size_t> configured{0};
+    if (smem > 48 * 1024 && smem > configured.load()) {
         ALTOB_CUDA(cudaFuncSetAttribute(k_solve_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = smem;
+        size_t cur = configured.load();
+        while (cur < smem && !configured.compare_exchange_weak(cur, smem)) {
+        }
     }
     k_solve_setup<<<1, DN_THREADS, smem, st>>>(G, nmode, target, R, W, info);
     ALTOB_LAUNCH_CHECK();
@@ -391,11 +394,12 @@ altob_status apply_w(FT* U, u64 I, int R, const double* W, NormKind nk, double* 
     }
     if (I == 0) return ALTOB_OK;
     size_t smem = (size_t)(R * R + R) * sizeof(double);
-    static size_t configured[2] = {0, 0};
-    size_t& cfg = configured[sizeof(FT) == 8];
-    if (smem > 48 * 1024 && smem > cfg) {
+    static std::atomic<size_t> cfg{0};  // one per FT instantiation
+    if (smem > 48 * 1024 && smem > cfg.load()) {
         ALTOB_CUDA(cudaFuncSetAttribute(k_apply<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cfg = smem;
+        size_t cur = cfg.load();
+        while (cur < smem && !cfg.compare_exchange_weak(cur, smem)) {
+        }
     }
     k_apply<FT><<<dn_grid(I, (DN_THREADS / 32) * AP_RW * 8), DN_THREADS, smem, st>>>(U, I, R, W, (int)nk, colacc);
     ALTOB_LAUNCH_CHECK();

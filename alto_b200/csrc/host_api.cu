@@ -54,6 +54,7 @@ altob_status altob_cpd_als_host(altob_tensor* t, altob_dtype ftype, void* const*
     if (!t || !h_factors || !h_lambda) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (ftype != ALTOB_F64 && ftype != ALTOB_F32) return fail(ALTOB_ERR_ARG, "dtype must be F64 or F32");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
     DevModel m;
     ALTOB_TRY(upload(t, fsz, h_factors, h_lambda, rank, m, st));
@@ -68,6 +69,7 @@ altob_status altob_cp_apr_host(altob_tensor* t, altob_dtype ftype, void* const* 
     if (!t || !h_factors || !h_lambda) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (ftype != ALTOB_F64 && ftype != ALTOB_F32) return fail(ALTOB_ERR_ARG, "dtype must be F64 or F32");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
     DevModel m;
     ALTOB_TRY(upload(t, fsz, h_factors, h_lambda, rank, m, st));

@@ -225,7 +225,15 @@ inline KeySrc key_src(const altob_tensor* t)
 }
 inline u64 fib_reuse(const altob_tensor* t, int n) { return t->nnz / t->dims[n]; }
 
-// Device allocation helpers that record failures as ALTOB_ERR_NOMEM.
+// Device allocation helpers that record failures as ALTOB_ERR_NOMEM.  They
+// use the stream-ordered allocator on the stream of the entry point that is
+// running on this thread (StreamScope), so freeing never waits for work on
+// other streams.
+struct StreamScope {
+    cudaStream_t prev;
+    explicit StreamScope(cudaStream_t s);
+    ~StreamScope();
+};
 altob_status dmalloc(void** p, size_t bytes);
 template <typename T>
 altob_status dmalloc_t(T** p, size_t count)

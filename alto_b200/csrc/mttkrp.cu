@@ -48,6 +48,28 @@ altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, 
         pl->lpn = std::max(2, std::min(32, next_pow2(lanes)));
         pl->ch = (int)((R + (u64)pl->lpn * pl->vec - 1) / ((u64)pl->lpn * pl->vec));
     }
+    pl->grouped = env_int("ALTOB_KERNEL", 4) == 4;
+    if (pl->grouped && pl->vec > 1) {
+        // fewer lanes per nonzero, two chunks each: amortizes per-nonzero work
+        const int want = env_int("ALTOB_LPN", 0);
+        if (want == 4 || want == 8 || want == 16) {
+            const u64 per = (u64)want * pl->vec;
+            const u64 ch = (R + per - 1) / per;
+            if (ch <= 2) {
+                pl->lpn = want;
+                pl->ch = (int)ch;
+            }
+        }
+    }
+    if (pl->grouped) {
+        // k_grouped: fixed tile, slot table only (no accumulator rows)
+        pl->tile = GT_TILE;
+        const int slots = env_int("ALTOB_GROUP_SLOTS", 2048);
+        pl->hslots = cache ? std::max(32, std::min(floor_pow2(slots), 8192)) : 0;
+        const int mm = t->nmode == 3 ? 3 : ALTOB_MAX_MODES;
+        pl->smem = grouped_smem(pl->hslots, mm, fsz);
+        return ALTOB_OK;
+    }
     pl->tile = env_int("ALTOB_TILE", 1024);
     pl->tile = std::max(256, (pl->tile / 256) * 256);
     int cache_bytes = env_int("ALTOB_CACHE_BYTES", 32 * 1024);
@@ -85,6 +107,7 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     c.lpn = pl.lpn;
     c.vec = pl.vec;
     c.ch = pl.ch;
+    c.grouped = pl.grouped;
     c.phi = phi ? 1 : 0;
     c.smem = pl.smem;
     c.grid = dim3(0);
@@ -213,12 +236,14 @@ extern "C" {
 altob_status altob_mttkrp(altob_tensor* t, int mode, altob_dtype ftype, void* const* d_factors, uint64_t rank,
                           int accumulate, altob_algo algo, void* stream)
 {
+    StreamScope scope((cudaStream_t)stream);
     return mttkrp_device(t, mode, ftype, d_factors, rank, accumulate, algo, (cudaStream_t)stream);
 }
 
 altob_status altob_phi(altob_tensor* t, int mode, altob_dtype ftype, void* const* d_factors, uint64_t rank,
                        double eps_div_zero, void* d_phi, void* stream)
 {
+    StreamScope scope((cudaStream_t)stream);
     return phi_device(t, mode, ftype, d_factors, rank, eps_div_zero, d_phi, (cudaStream_t)stream);
 }
 
@@ -228,6 +253,7 @@ altob_status altob_mttkrp_host(altob_tensor* t, int mode, altob_dtype ftype, voi
     if (!t || !h_factors) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
     void* d[ALTOB_MAX_MODES];
     altob_status s = upload_factors(t, h_factors, fsz, rank, d, st);
@@ -247,6 +273,7 @@ altob_status altob_mttkrp_sweep_host(altob_tensor* t, altob_dtype ftype, void* c
 {
     if (!t || !h_factors) return fail(ALTOB_ERR_ARG, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
     const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
     void* d[ALTOB_MAX_MODES];
     altob_status s = upload_factors(t, h_factors, fsz, rank, d, st);

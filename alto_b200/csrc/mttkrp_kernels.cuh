@@ -399,6 +399,406 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
     }
 }
 
+// ---------------------------------------------------------------- k_grouped
+//
+// Second MTTKRP / Phi kernel: no shared-memory accumulators at all.  Per tile
+// of GT_TILE nonzeros:
+//   A1  load keys and values (coalesced), write one record per nonzero
+//       (mode indices + value) to shared memory, claim a slot for the output
+//       row in a direct-mapped tag table, and take a rank inside the slot
+//       with one atomic per group of equal slots in a warp (match_any);
+//   A2  exclusive scan of the slot counts in claim order;
+//   A3  scatter the nonzero numbers into slot order (a counting sort), so
+//       nonzeros with the same output row are contiguous;
+//   B   each lane group walks a contiguous range of the sorted list, gathers
+//       the other modes' rows, keeps the running sum of equal output rows in
+//       registers and adds each finished run to global memory with one
+//       vector atomic.
+// Nonzeros whose slot is held by another row form single-element runs.
+// The run is the reference's fiber and the flush its pull.
+
+constexpr int GT_TILE = 1024;
+constexpr int GT_IPT = GT_TILE / MT_THREADS;
+
+// 32-bit words of one shared record: output index, the other modes' indices,
+// the value, padding to 16 B.
+template <typename FT, int MM>
+struct RecWords {
+    static constexpr int n = (MM + (int)(sizeof(FT) / 4) + 3) & ~3;
+};
+
+inline size_t grouped_smem(int hslots, int mm, size_t fsz)
+{
+    const int rw = (mm + (int)(fsz / 4) + 3) & ~3;
+    size_t b = (size_t)GT_TILE * rw * 4 * 2;  // records, then records in run order
+    b += (size_t)hslots * 8;                  // tags + counts
+    b += (size_t)GT_TILE * 4;                 // claimed-slot list
+    return b;
+}
+
+template <typename FT, int RW>
+__device__ __forceinline__ void load_rec(const u32* r, u32* w)
+{
+#pragma unroll
+    for (int w4 = 0; w4 < RW; w4 += 4) {
+        const uint4 t4 = *reinterpret_cast<const uint4*>(r + w4);
+        w[w4] = t4.x;
+        w[w4 + 1] = t4.y;
+        w[w4 + 2] = t4.z;
+        w[w4 + 3] = t4.w;
+    }
+}
+
+template <typename FT, int MM>
+__device__ __forceinline__ FT rec_val(const u32* w)
+{
+    if constexpr (sizeof(FT) == 4) return (FT)__uint_as_float(w[MM]);
+    else return (FT)__longlong_as_double((long long)(((unsigned long long)w[MM + 1] << 32) | w[MM]));
+}
+
+template <typename FT, int VEC, int CH, int LPN>
+__device__ __forceinline__ void flush_run(FT* out, u32 row, int R, int sub, FT (*racc)[VEC])
+{
+#pragma unroll
+    for (int ch = 0; ch < CH; ++ch) {
+        const int r0 = ch * LPN * VEC + sub * VEC;
+        if (r0 < R) gred<FT, VEC>(out + (size_t)row * R + r0, racc[ch]);
+    }
+}
+
+// One nonzero of a lane group: val * (Khatri-Rao row of the other modes), or
+// the Phi contribution.  Record words: [target index, other indices..., value].
+template <typename FT, int MM, int NM, int LPN, int VEC, int CH, bool PHI>
+__device__ __forceinline__ void nz_row(const u32* w, const FT* const* Uo, const FT* Ut, int R, int sub, int nother,
+                                       FT eps, unsigned gmask, FT (*x)[VEC])
+{
+    const FT v = rec_val<FT, MM>(w);
+#pragma unroll
+    for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) x[ch][e] = PHI ? FT(1) : v;
+    FT y[MM - 1][CH][VEC];
+#pragma unroll
+    for (int k = 0; k < MM - 1; ++k) {
+        if (NM == 0 && k >= nother) break;
+        const FT* row = Uo[k] + (size_t)w[1 + k] * R;
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+            const int r0 = ch * LPN * VEC + sub * VEC;
+            if (r0 < R) vload<FT, VEC>(row + r0, y[k][ch]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < MM - 1; ++k) {
+        if (NM == 0 && k >= nother) break;
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+            const int r0 = ch * LPN * VEC + sub * VEC;
+            if (r0 < R) vmul<FT, VEC>(x[ch], y[k][ch]);
+        }
+    }
+    if constexpr (PHI) {
+        const FT* brow = Ut + (size_t)w[0] * R;
+        FT dot = FT(0);
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+            const int r0 = ch * LPN * VEC + sub * VEC;
+            if (r0 < R) {
+                FT b[VEC];
+                vload<FT, VEC>(brow + r0, b);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) dot += b[e] * x[ch][e];
+            }
+        }
+#pragma unroll
+        for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(gmask, dot, o, LPN);
+        const FT sc = v / (dot > eps ? dot : eps);
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) x[ch][e] *= sc;
+    }
+}
+
+template <typename FT, int VEC, int CH>
+__device__ __forceinline__ void run_add(FT (*racc)[VEC], FT (*x)[VEC])
+{
+#pragma unroll
+    for (int ch = 0; ch < CH; ++ch) {
+        if constexpr (sizeof(FT) == 4 && VEC % 2 == 0) {
+#pragma unroll
+            for (int e = 0; e < VEC; e += 2) {
+                const float2 r = __fadd2_rn(make_float2(racc[ch][e], racc[ch][e + 1]), make_float2(x[ch][e], x[ch][e + 1]));
+                racc[ch][e] = r.x;
+                racc[ch][e + 1] = r.y;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) racc[ch][e] += x[ch][e];
+        }
+    }
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
+{
+    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    constexpr int NPW = 32 / LPN;
+    constexpr int RW = RecWords<FT, MM>::n;
+    constexpr int NGRP = MT_WARPS * NPW;
+    constexpr int IPG = GT_TILE / NGRP;  // sorted nonzeros per lane group
+    constexpr int FW = (int)(sizeof(FT) / 4);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int R = a.R, H = a.hslots;
+    const int nmode = NM ? NM : a.nmode;
+    u32* rec = reinterpret_cast<u32*>(smem);
+    u32* srec = rec + (size_t)GT_TILE * RW;  // records in run order
+    u32* tag = srec + (size_t)GT_TILE * RW;
+    u32* cnt = tag + H;
+    u32* used = cnt + H;
+    __shared__ u32 nused, ndirect, wsum[MT_WARPS];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = tid; k < H; k += MT_THREADS) {
+        tag[k] = 0;
+        cnt[k] = 0;
+    }
+    if (tid == 0) {
+        nused = 0;
+        ndirect = 0;
+    }
+    __syncthreads();
+
+    const VT* vals = reinterpret_cast<const VT*>(a.vals);
+    const int target = a.target;
+    const int sub = lane % LPN, q = lane / LPN;
+    const int grp = warp * NPW + q;
+    const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
+    const u32 lt_mask = (1u << lane) - 1u;
+    const FT* Uo[MM - 1];
+#pragma unroll
+    for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : (k + 1 < MM ? k + 1 : k)];
+    const FT* Ut = a.U[target];
+    const int nother = nmode - 1;
+
+    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) {
+        const u64 g0 = ti * (u64)GT_TILE;
+        const int nvalid = (int)min((u64)GT_TILE, a.nnz - g0);
+        u64 hcur = 0, hnext = 0, nstart = ~0ull;
+        bool slow_hi = a.perm != nullptr;
+        if (!a.key.khi && a.key.nrun && !slow_hi) {
+            const int r = run_of(a.key, g0);
+            hcur = a.key.run_val[r];
+            if (r + 1 < a.key.nrun) {
+                nstart = a.key.run_start[r + 1];
+                hnext = a.key.run_val[r + 1];
+                if (r + 2 < a.key.nrun && a.key.run_start[r + 2] < g0 + (u64)GT_TILE) slow_hi = true;
+            }
+        }
+        // ---- A1: records [target, others..., value], slot claims, ranks
+        u64 lo[GT_IPT], posv[GT_IPT];
+        VT vv[GT_IPT];
+#pragma unroll
+        for (int k = 0; k < GT_IPT; ++k) {
+            const int it = tid + k * MT_THREADS;
+            const u64 g = g0 + it;
+            posv[k] = 0;
+            if (it < nvalid) {
+                const u64 pos = a.perm ? (u64)a.perm[g] : g;
+                posv[k] = pos;
+                lo[k] = a.key.klo[pos];
+                vv[k] = vals[pos];
+            }
+        }
+        int slv[GT_IPT];
+        u32 rankv[GT_IPT];
+#pragma unroll
+        for (int k = 0; k < GT_IPT; ++k) {
+            const int it = tid + k * MT_THREADS;
+            const u64 g = g0 + it;
+            int sl = -2;
+            bool claimed = false;
+            u32 h = 0;
+            if (it < nvalid) {
+                u64 hi;
+                if (a.key.khi) hi = a.key.khi[posv[k]];
+                else if (a.key.nrun == 0) hi = 0;
+                else if (slow_hi) hi = key_hi(a.key, posv[k]);
+                else hi = g >= nstart ? hnext : hcur;
+                u32* r = rec + (size_t)it * RW;
+                u32 trow = 0;
+#pragma unroll
+                for (int m = 0; m < MM; ++m) {
+                    if (NM == 0 && m >= nmode) break;
+                    const u32 c = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
+                    r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
+                    if (m == target) trow = c;
+                }
+                const FT fv = (FT)vv[k];
+                if constexpr (FW == 1) {
+                    r[MM] = __float_as_uint((float)fv);
+                } else {
+                    const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
+                    r[MM] = (u32)b;
+                    r[MM + 1] = (u32)(b >> 32);
+                }
+                sl = -1;
+                if (H) {
+                    h = trow & (u32)(H - 1);
+                    const u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
+                    if (old == 0u) {
+                        claimed = true;
+                        sl = (int)h;
+                    } else if (old == trow + 1u) {
+                        sl = (int)h;
+                    }
+                }
+            }
+            const u32 cm = __ballot_sync(0xffffffffu, claimed);
+            if (cm) {
+                u32 base = 0;
+                if (lane == 0) base = atomicAdd(&nused, (u32)__popc(cm));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (claimed) used[base + __popc(cm & lt_mask)] = h;
+            }
+            const u32 key = sl >= 0 ? (u32)sl : (0x80000000u | (u32)lane);
+            const u32 peers = __match_any_sync(0xffffffffu, key);
+            const int leader = __ffs(peers) - 1;
+            u32 base = 0;
+            if (sl >= 0 && lane == leader) base = atomicAdd(&cnt[sl], (u32)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            u32 rank = base + __popc(peers & lt_mask);
+            const u32 dm = __ballot_sync(0xffffffffu, sl == -1);
+            if (dm) {
+                u32 db = 0;
+                if (lane == 0) db = atomicAdd(&ndirect, (u32)__popc(dm));
+                db = __shfl_sync(0xffffffffu, db, 0);
+                if (sl == -1) rank = db + __popc(dm & lt_mask);
+            }
+            slv[k] = sl;
+            rankv[k] = rank;
+        }
+        __syncthreads();
+        // ---- A2: exclusive scan of the counts in claim order
+        const u32 nu = nused;
+        {
+            u32 c[GT_IPT], sum = 0;
+#pragma unroll
+            for (int k = 0; k < GT_IPT; ++k) {
+                const u32 e = (u32)(tid * GT_IPT + k);
+                c[k] = e < nu ? cnt[used[e]] : 0u;
+                sum += c[k];
+            }
+            u32 xs = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 y = __shfl_up_sync(0xffffffffu, xs, o);
+                if (lane >= o) xs += y;
+            }
+            if (lane == 31) wsum[warp] = xs;
+            __syncthreads();
+            u32 wbase = 0;
+#pragma unroll
+            for (int w = 0; w < MT_WARPS; ++w)
+                if (w < warp) wbase += wsum[w];
+            u32 run = wbase + xs - sum;
+#pragma unroll
+            for (int k = 0; k < GT_IPT; ++k) {
+                const u32 e = (u32)(tid * GT_IPT + k);
+                if (e < nu) {
+                    const u32 hh = used[e];
+                    tag[hh] = 0;    // tags are not read again in this tile
+                    cnt[hh] = run;  // count -> start offset
+                }
+                run += c[k];
+            }
+        }
+        __syncthreads();
+        // ---- A3: records into run order (counting-sort scatter)
+        u32 slotted = 0;
+#pragma unroll
+        for (int w = 0; w < MT_WARPS; ++w) slotted += wsum[w];
+#pragma unroll
+        for (int k = 0; k < GT_IPT; ++k) {
+            const int it = tid + k * MT_THREADS;
+            if (it < nvalid) {
+                const int sl = slv[k];
+                const u32 pos = sl >= 0 ? cnt[sl] + rankv[k] : slotted + rankv[k];
+                const u32* src = rec + (size_t)it * RW;
+                u32* dst = srec + (size_t)pos * RW;
+#pragma unroll
+                for (int w4 = 0; w4 < RW; w4 += 4)
+                    *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
+            }
+        }
+        __syncthreads();
+        // ---- B: runs of equal output rows, one atomic per run
+        u32 prow = 0xffffffffu;
+        FT racc[CH][VEC];
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) racc[ch][e] = FT(0);
+        const int p0 = grp * IPG;
+        const int pend = min(p0 + IPG, nvalid);
+        int p = p0;
+        // two nonzeros per step: both gathers in flight before the run logic
+        for (; p + 1 < pend; p += 2) {
+            u32 w0[RW], w1[RW];
+            load_rec<FT, RW>(srec + (size_t)p * RW, w0);
+            load_rec<FT, RW>(srec + (size_t)(p + 1) * RW, w1);
+            FT x0[CH][VEC], x1[CH][VEC];
+            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
+            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w1, Uo, Ut, R, sub, nother, a.eps, gmask, x1);
+            if (w0[0] != prow) {
+                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+                prow = w0[0];
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
+            } else {
+                run_add<FT, VEC, CH>(racc, x0);
+            }
+            if (w1[0] != prow) {
+                flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+                prow = w1[0];
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x1[ch][e];
+            } else {
+                run_add<FT, VEC, CH>(racc, x1);
+            }
+        }
+        if (p < pend) {
+            u32 w0[RW];
+            load_rec<FT, RW>(srec + (size_t)p * RW, w0);
+            FT x0[CH][VEC];
+            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
+            if (w0[0] != prow) {
+                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+                prow = w0[0];
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
+            } else {
+                run_add<FT, VEC, CH>(racc, x0);
+            }
+        }
+        if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+        __syncthreads();
+        // counts back to zero for the next tile (tags were cleared in A2)
+        for (u32 e = tid; e < nu; e += MT_THREADS) cnt[used[e]] = 0;
+        if (tid == 0) {
+            nused = 0;
+            ndirect = 0;
+        }
+        __syncthreads();
+    }
+}
+
 template <typename FT>
 struct CrArgsK {
     KeySrc key;

@@ -3,12 +3,15 @@
 // (mttkrp_<ft>_<vt>.cu) so the kernels compile in parallel.
 #pragma once
 
+#include <atomic>
+
 #include "mttkrp_kernels.cuh"
 
 namespace altob {
 
 struct TiledCfg {
     int lpn, vec, ch, phi;
+    int grouped;  // 1: k_grouped, 0: k_tiled
     dim3 grid;
     size_t smem;
 };
@@ -21,15 +24,16 @@ altob_status launch_atomic_cr(const CrArgsK<FT>& a, cudaStream_t st);
 
 // Sets the kernel's shared-memory limit once and launches it (or only
 // reports occupancy when grid.x == 0).
-template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+template <typename K>
+altob_status launch_kernel(K k, std::atomic<size_t>& configured, const void* args_ptr, const TiledCfg& c,
+                           cudaStream_t st, int* bps)
 {
-    auto k = k_tiled<FT, VT, NM, LPN, VEC, CH, PHI>;
-    static size_t configured = 0;
-    if (c.smem > configured) {
+    if (c.smem > configured.load()) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem);
         if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("smem attribute: ") + cudaGetErrorString(e));
-        configured = c.smem;
+        size_t cur = configured.load();
+        while (cur < c.smem && !configured.compare_exchange_weak(cur, c.smem)) {
+        }
     }
     if (bps) {
         int n = 0;
@@ -37,10 +41,25 @@ altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t 
         *bps = n;
     }
     if (c.grid.x == 0) return ALTOB_OK;
-    k<<<c.grid, MT_THREADS, c.smem, st>>>(a);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("k_tiled launch: ") + cudaGetErrorString(e));
+    void* args[] = {const_cast<void*>(args_ptr)};
+    cudaError_t e = cudaLaunchKernel((const void*)k, c.grid, dim3(MT_THREADS), args, c.smem, st);
+    if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("MTTKRP launch: ") + cudaGetErrorString(e));
     return ALTOB_OK;
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+altob_status launch_grouped(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    static std::atomic<size_t> configured{0};
+    return launch_kernel(k_grouped<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    if (c.grouped) return launch_grouped<FT, VT, NM, LPN, VEC, CH, PHI>(a, c, st, bps);
+    static std::atomic<size_t> configured{0};
+    return launch_kernel(k_tiled<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
 }
 
 // (lanes per nonzero, elements per lane, chunks) -> kernel
@@ -49,7 +68,16 @@ altob_status launch_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
 {
     constexpr int V = 16 / sizeof(FT);
     if (c.vec == 1) return launch_one<FT, VT, NM, 32, 1, 4, PHI>(a, c, st, bps);
-    if (c.ch == 2) return launch_one<FT, VT, NM, 32, V, 2, PHI>(a, c, st, bps);
+    if (c.ch == 2) {
+        if (c.lpn == 32) return launch_one<FT, VT, NM, 32, V, 2, PHI>(a, c, st, bps);
+        if (!c.grouped) return fail(ALTOB_ERR_UNSUPPORTED, "shape needs the grouped kernel");
+        switch (c.lpn) {
+        case 4: return launch_grouped<FT, VT, NM, 4, V, 2, PHI>(a, c, st, bps);
+        case 8: return launch_grouped<FT, VT, NM, 8, V, 2, PHI>(a, c, st, bps);
+        case 16: return launch_grouped<FT, VT, NM, 16, V, 2, PHI>(a, c, st, bps);
+        }
+        return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
+    }
     switch (c.lpn) {
     case 2: return launch_one<FT, VT, NM, 2, V, 1, PHI>(a, c, st, bps);
     case 4: return launch_one<FT, VT, NM, 4, V, 1, PHI>(a, c, st, bps);

@@ -6,7 +6,7 @@
 namespace altob {
 
 struct TiledPlan {
-    int vec, lpn, ch, tile, hslots;
+    int vec, lpn, ch, tile, hslots, grouped;
     size_t smem;
 };
 
