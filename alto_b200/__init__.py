@@ -30,6 +30,8 @@ _DT = {"f64": F64, "float64": F64, "f32": F32, "float32": F32, "u32": U32, "uint
 _NP = {F64: np.float64, F32: np.float32, U32: np.uint32}
 ALGOS = {"auto": 0, "tiled": 1, "atomic": 2, "atomic_cr": 3, "op_sched": 4}
 MAX_MODES = 5
+# altob_status codes (include/altob.h)
+OK, ERR_ARG, ERR_BITS, ERR_CUDA, ERR_NOMEM, ERR_IO, ERR_UNSUPPORTED, ERR_NOT_FOUND = range(8)
 
 
 class AltobError(RuntimeError):
@@ -84,6 +86,11 @@ SIGNATURES = {
     "altob_cpd_als_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _d, _dp, C.POINTER(_i), _vp]),
     "altob_cp_apr_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _i, _d, _d, _d, _d, _i, _dp, _vp]),
     "altob_kruskal_random_init": (_i, [_i, _u64p, _u64, C.c_uint, _i, _vp, _vp]),
+    "altob_batch_create": (_i, [_vp, _i, _u64p, _i, _vp, _vp, _i, _vp, C.POINTER(_vp)]),
+    "altob_batch_autotune": (_i, [_vp, _vp]),
+    "altob_batch_cpd_als": (_i, [_vp, _i, _d, _dp, C.POINTER(_i), _i, _vp]),
+    "altob_batch_describe": (_i, [_vp, C.c_char_p, C.c_size_t]),
+    "altob_batch_destroy": (_i, [_vp]),
 }
 
 
@@ -432,6 +439,65 @@ def tt_logLikelihood(at: AltoTensor, M: KruskalModel, eps_div_zero=1e-10, stream
     _check(lib().altob_loglik(at.handle, ft, _ptr_array(ptrs), _dev_ptr(M.lam), M.rank, float(eps_div_zero),
                               C.byref(ll), _stream_ptr(stream)))
     return ll.value
+
+
+class BatchCPD:
+    """Many independent CP-ALS solves in batched launches (no counterpart in
+    the reference; each tensor follows cpd_alto, include/cpd.hpp:43-186).
+
+    tensors: AltoTensor handles; models: KruskalModel with CUDA tensors (all
+    FP32 or all FP64).  The models are updated in place by every solve().
+    The handle keeps references to both so their memory outlives it."""
+
+    def __init__(self, tensors, models, fit_capacity=64, stream=None):
+        if len(tensors) != len(models) or not tensors:
+            raise ValueError("need one model per tensor")
+        ft = _ftype_of(models[0].U)
+        self._tensors, self._models = list(tensors), list(models)
+        self.count = len(tensors)
+        self.fit_capacity = int(fit_capacity)
+        n = self.count
+        th = (C.c_void_p * n)(*[t.handle for t in tensors])
+        ranks = (C.c_uint64 * n)(*[m.rank for m in models])
+        self._rows = []
+        for m in models:
+            if _ftype_of(m.U) != ft:
+                raise ValueError("all models need one dtype")
+            self._rows.append(_ptr_array([_dev_ptr(u) for u in m.U]))
+        fac = (C.c_void_p * n)(*[C.cast(r, C.c_void_p).value for r in self._rows])
+        lam = (C.c_void_p * n)(*[_dev_ptr(m.lam) for m in models])
+        h = C.c_void_p()
+        _check(lib().altob_batch_create(th, n, ranks, ft, fac, lam, self.fit_capacity, _stream_ptr(stream),
+                                        C.byref(h)))
+        self.handle = h.value
+
+    def autotune(self, stream=None):
+        _check(lib().altob_batch_autotune(self.handle, _stream_ptr(stream)))
+
+    def solve(self, max_iters, epsilon, use_graph=True, stream=None):
+        """Returns (fits[count, max_iters], iters[count])."""
+        fits = np.zeros((self.count, max_iters))
+        iters = np.zeros(self.count, dtype=np.int32)
+        _check(lib().altob_batch_cpd_als(self.handle, int(max_iters), float(epsilon), fits.ctypes.data_as(_dp),
+                                         iters.ctypes.data_as(C.POINTER(_i)), int(bool(use_graph)),
+                                         _stream_ptr(stream)))
+        return fits, iters
+
+    def describe(self):
+        buf = C.create_string_buffer(1 << 16)
+        _check(lib().altob_batch_describe(self.handle, buf, len(buf)))
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().altob_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def status_of(fn, *args):

@@ -18,8 +18,6 @@
 
 namespace altob {
 
-altob_status check_model(const altob_tensor* t, altob_dtype ft, void* const* dU, u64 rank);
-
 // |min(B, 1 - Phi)| max-reduced (apr.hpp:1210-1216); with `mult`, also
 // B *= Phi (apr.hpp:1226-1231) in the same pass.
 template <typename FT>

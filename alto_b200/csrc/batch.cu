@@ -1,0 +1,771 @@
+// batch.cu -- many independent CP-ALS solves in batched launches.
+//
+// No counterpart in the reference (it decomposes one tensor per process).
+// Every tensor of the batch keeps its own device model and follows exactly
+// the per-tensor algorithm of cpd_alto (include/cpd.hpp:43-186, as in
+// cpd.cu), but each step runs for all tensors in one launch:
+//   zero U_j | MTTKRP (one launch per shape class) | copy of the last mode |
+//   prepare | R x R solve (one CTA per tensor) | row apply + column norms |
+//   lambda | Gram of the normalised factor  -- for every mode j --
+//   then the fit, which also records the per-iteration fit and clears the
+//   tensor's active flag when |fit - prev| < epsilon or max_iters is reached.
+// Inactive tensors are skipped by every kernel, so a tensor's result equals
+// its stand-alone solve.  Iterations after the first are captured once as a
+// CUDA graph and replayed.  A shape class is (order 3 or other, lanes per
+// nonzero, elements per lane, value type); its slot count and lane layout are
+// picked by altob_batch_autotune.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "dense_kernels.cuh"
+#include "mttkrp_launch.cuh"
+#include "mttkrp_plan.h"
+
+namespace altob {
+
+template <typename FT>
+struct BDesc {
+    FT* U[ALTOB_MAX_MODES];
+    u64 dims[ALTOB_MAX_MODES];
+    int nmode, R;
+    double *G, *W, *colacc, *lam, *inner, *fit_tmp, *fits;
+    FT* M;
+    FT* lam_out;
+    double normAT;
+    int* info;
+};
+
+// ------------------------------------------------------------ kernels
+
+template <typename FT>
+__global__ void k_b_zero(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
+                         const int* __restrict__ active, int j)
+{
+    const int b = list[blockIdx.y];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    const u64 n = t.dims[j] * (u64)t.R;
+    FT* U = t.U[j];
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x) U[e] = FT(0);
+}
+
+template <typename FT>
+__global__ void k_b_copym(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
+                          const int* __restrict__ active, int j)
+{
+    const int b = list[blockIdx.y];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    if (j != t.nmode - 1) return;
+    const u64 n = t.dims[j] * (u64)t.R;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x)
+        t.M[e] = t.U[j][e];
+}
+
+template <typename FT>
+__global__ void k_b_prep(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
+                         const int* __restrict__ active, int j, int nk)
+{
+    const int b = list[blockIdx.x];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    const int R = t.R;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        t.colacc[r] = nk == NORM_MAX ? 1.0 : 0.0;
+        if (j == t.nmode - 1) t.inner[r] = 0.0;
+    }
+    double* G = t.G + (size_t)j * R * R;
+    for (int e = threadIdx.x; e < R * R; e += blockDim.x) G[e] = 0.0;
+}
+
+template <typename FT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_solve(const BDesc<FT>* __restrict__ d,
+                                                        const int* __restrict__ list,
+                                                        const int* __restrict__ active, int j)
+{
+    const int b = list[blockIdx.x];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    solve_body(t.G, t.nmode, j, t.R, t.W, t.info);
+}
+
+template <typename FT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_apply(const BDesc<FT>* __restrict__ d,
+                                                        const int* __restrict__ list,
+                                                        const int* __restrict__ active, int j, int nk)
+{
+    const int b = list[blockIdx.y];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    apply_body<FT>(t.U[j], t.dims[j], t.R, t.W, nk, t.colacc, blockIdx.x, gridDim.x);
+}
+
+template <typename FT>
+__global__ void k_b_lambda(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
+                           const int* __restrict__ active, int nk)
+{
+    const int b = list[blockIdx.x];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    for (int r = threadIdx.x; r < t.R; r += blockDim.x) t.lam[r] = nk == NORM_2 ? sqrt(t.colacc[r]) : t.colacc[r];
+}
+
+// Gram of U_j; with `scaled`, U_j /= lambda first (written back) and the
+// fit's inner product with the saved MTTKRP of the last mode.
+template <typename FT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_gram(const BDesc<FT>* __restrict__ d,
+                                                       const int* __restrict__ list,
+                                                       const int* __restrict__ active, int j, int scaled)
+{
+    const int b = list[blockIdx.y];
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    const int R = t.R;
+    const bool last = j == t.nmode - 1;
+    gram_body<FT>(t.U[j], t.dims[j], R, t.G + (size_t)j * R * R, scaled ? t.lam : nullptr,
+                  scaled ? t.U[j] : nullptr, (scaled && last) ? t.M : nullptr, t.inner, blockIdx.x, gridDim.x);
+}
+
+template <typename FT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_fit(const BDesc<FT>* __restrict__ d, int* __restrict__ active,
+                                                      int* __restrict__ iters, double eps, int max_iters)
+{
+    const int b = blockIdx.x;
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    fit_body(t.G, t.nmode, t.R, t.lam, t.inner, t.normAT, t.fit_tmp);
+    if (threadIdx.x == 0) {
+        const double f = *t.fit_tmp;
+        const int it = iters[b];
+        t.fits[it] = f;
+        iters[b] = it + 1;
+        if ((it > 0 && fabs(t.fits[it - 1] - f) < eps) || it + 1 >= max_iters) active[b] = 0;
+    }
+}
+
+template <typename FT>
+__global__ void k_b_lamout(const BDesc<FT>* __restrict__ d, int count)
+{
+    const int b = blockIdx.x;
+    if (b >= count) return;
+    const BDesc<FT>& t = d[b];
+    if (!t.lam_out) return;
+    for (int r = threadIdx.x; r < t.R; r += blockDim.x) t.lam_out[r] = (FT)t.lam[r];
+}
+
+template <typename FT, typename VT>
+__global__ void k_b_sumsq(BDesc<FT>* __restrict__ d, const void* const* __restrict__ vals,
+                          const u64* __restrict__ nnz)
+{
+    const int b = blockIdx.y;
+    const VT* v = reinterpret_cast<const VT*>(vals[b]);
+    double s = 0.0;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < nnz[b]; e += (u64)gridDim.x * blockDim.x) {
+        const double x = (double)v[e];
+        s += x * x;
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&d[b].normAT, s);
+}
+
+// ---------------------------------------------------------------- host
+
+template <typename FT>
+struct ClassRun {
+    int nm = 0;  // 3 or 0 (order 4-5)
+    altob_dtype vdt = ALTOB_F32;
+    int lpn = 32, vec = 1, ch = 4;
+    int hslots = 0;      // row slots of the grouped kernel (0: no grouping)
+    unsigned gridx = 1;  // resident CTAs for the current choice
+    size_t smem = 0;
+    std::vector<int> members;  // batch indices
+    int mode_count[ALTOB_MAX_MODES] = {0};
+    TiledArgs<FT>* d_args[ALTOB_MAX_MODES] = {nullptr};
+    u64* d_prefix[ALTOB_MAX_MODES] = {nullptr};
+    int* d_bid[ALTOB_MAX_MODES] = {nullptr};
+    u64 total_tiles[ALTOB_MAX_MODES] = {0};
+    std::string key;
+    float tuned_ms = -1.f;
+
+    TiledCfg cfg(unsigned gx) const
+    {
+        TiledCfg c;
+        c.lpn = lpn;
+        c.vec = vec;
+        c.ch = ch;
+        c.phi = 0;
+        c.grouped = 1;
+        c.grid = dim3(gx);
+        c.smem = smem;
+        return c;
+    }
+    void free_args()
+    {
+        for (int j = 0; j < ALTOB_MAX_MODES; ++j) {
+            dfree(d_args[j]);
+            dfree(d_prefix[j]);
+            dfree(d_bid[j]);
+            d_args[j] = nullptr;
+            d_prefix[j] = nullptr;
+            d_bid[j] = nullptr;
+            total_tiles[j] = 0;
+        }
+    }
+};
+
+struct BatchBase {
+    virtual ~BatchBase() {}
+    virtual altob_status autotune(cudaStream_t st) = 0;
+    virtual altob_status solve(int max_iters, double eps, double* fits, int* iters, int use_graph,
+                               cudaStream_t st) = 0;
+    virtual void describe(std::string* out) const = 0;
+};
+
+template <typename FT>
+struct BatchImpl : BatchBase {
+    int count = 0, maxN = 0, maxR = 0, cap = 0;
+    std::vector<altob_tensor*> ts;
+    std::vector<BDesc<FT>> hdesc;
+    BDesc<FT>* d_desc = nullptr;
+    int* d_active = nullptr;
+    int* d_iters = nullptr;
+    int* d_list[ALTOB_MAX_MODES] = {nullptr};
+    int nlist[ALTOB_MAX_MODES] = {0};
+    void* d_scratch = nullptr;
+    std::vector<std::unique_ptr<ClassRun<FT>>> classes;
+    cudaStream_t cap_stream = nullptr;  // graph capture (never the legacy stream)
+    cudaGraphExec_t gexec = nullptr;
+    double g_eps = -1.0;
+    int g_iters = -1;
+    int gx_apply = 1, gx_elem = 1;
+
+    ~BatchImpl() override
+    {
+        StreamScope scope(0);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        dfree(d_desc);
+        dfree(d_active);
+        dfree(d_iters);
+        for (int j = 0; j < ALTOB_MAX_MODES; ++j) dfree(d_list[j]);
+        dfree(d_scratch);
+        for (auto& c : classes) c->free_args();
+    }
+
+    void drop_graph()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+    }
+
+    altob_status launch_mt(const ClassRun<FT>& c, const BatchTiles<FT>& bt, const TiledCfg& cfg, cudaStream_t st,
+                           int* bps)
+    {
+        if (c.vdt == ALTOB_U32) return launch_batch<FT, u32>(bt, c.nm, cfg, st, bps);
+        return launch_batch<FT, FT>(bt, c.nm, cfg, st, bps);
+    }
+
+    // Per-mode argument tables of a class for its current slot count.
+    altob_status build_class_args(ClassRun<FT>& c, cudaStream_t st)
+    {
+        c.free_args();
+        for (int j = 0; j < maxN; ++j) {
+            std::vector<TiledArgs<FT>> args;
+            std::vector<u64> prefix;
+            std::vector<int> bid;
+            u64 tiles = 0;
+            for (int b : c.members) {
+                altob_tensor* t = ts[b];
+                if (t->nmode <= j) continue;
+                TiledArgs<FT> a;
+                memset(&a, 0, sizeof(a));
+                a.key = key_src(t);
+                a.vals = t->d_vals;
+                // low fiber reuse: read in the target mode's order (oidx), as
+                // the reference's op_sched dispatch does (alto.hpp:637-664)
+                a.perm = (fib_reuse(t, j) <= 4 && t->d_oidx[j]) ? t->d_oidx[j] : nullptr;
+                a.nnz = t->nnz;
+                a.ntiles = (t->nnz + GT_TILE - 1) / GT_TILE;
+                a.nmode = t->nmode;
+                a.target = j;
+                a.R = hdesc[b].R;
+                a.tile = GT_TILE;
+                a.hslots = c.hslots;
+                a.eps = FT(0);
+                for (int m = 0; m < t->nmode; ++m) a.U[m] = hdesc[b].U[m];
+                a.out = hdesc[b].U[j];
+                a.fld = t->fld;
+                args.push_back(a);
+                prefix.push_back(tiles);
+                bid.push_back(b);
+                tiles += a.ntiles;
+            }
+            prefix.push_back(tiles);
+            c.mode_count[j] = (int)args.size();
+            c.total_tiles[j] = tiles;
+            if (args.empty()) continue;
+            ALTOB_TRY(dmalloc_t(&c.d_args[j], args.size()));
+            ALTOB_TRY(dmalloc_t(&c.d_prefix[j], prefix.size()));
+            ALTOB_TRY(dmalloc_t(&c.d_bid[j], bid.size()));
+            ALTOB_CUDA(cudaMemcpyAsync(c.d_args[j], args.data(), args.size() * sizeof(TiledArgs<FT>),
+                                       cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(c.d_prefix[j], prefix.data(), prefix.size() * sizeof(u64),
+                                       cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(c.d_bid[j], bid.data(), bid.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        }
+        ALTOB_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+        return ALTOB_OK;
+    }
+
+    // slot count and lane layout of a class -> argument tables and grid
+    altob_status set_choice(ClassRun<FT>& c, int hslots, int lpn, int ch, cudaStream_t st)
+    {
+        c.hslots = hslots;
+        c.lpn = lpn;
+        c.ch = ch;
+        c.smem = grouped_smem(hslots, c.nm == 3 ? 3 : ALTOB_MAX_MODES, sizeof(FT));
+        ALTOB_TRY(build_class_args(c, st));
+        BatchTiles<FT> bt;
+        memset(&bt, 0, sizeof(bt));
+        bt.hslots = hslots;
+        int bps = 0;
+        ALTOB_TRY(launch_mt(c, bt, c.cfg(0), st, &bps));  // sets the smem limit, reports occupancy
+        if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "batched MTTKRP kernel does not fit on an SM");
+        c.gridx = (unsigned)(bps * num_sms());
+        return ALTOB_OK;
+    }
+
+    altob_status mttkrp_class(ClassRun<FT>& c, int j, cudaStream_t st)
+    {
+        if (!c.d_args[j] || c.total_tiles[j] == 0) return ALTOB_OK;
+        BatchTiles<FT> bt;
+        bt.args = c.d_args[j];
+        bt.tile_prefix = c.d_prefix[j];
+        bt.bid = c.d_bid[j];
+        bt.active = d_active;
+        bt.ntensors = c.mode_count[j];
+        bt.hslots = c.hslots;
+        bt.total_tiles = c.total_tiles[j];
+        const unsigned gx = (unsigned)std::max<u64>(1, std::min<u64>(c.total_tiles[j], c.gridx));
+        return launch_mt(c, bt, c.cfg(gx), st, nullptr);
+    }
+
+    size_t smem_solve() const { return (size_t)2 * maxR * maxR * sizeof(double); }
+    size_t smem_apply() const { return (size_t)(maxR * maxR + maxR) * sizeof(double); }
+    size_t smem_gram() const { return (size_t)(GR_ROWS * maxR + maxR) * sizeof(double); }
+
+    // one CP-ALS iteration over all active tensors (cpd.hpp:96-160 per tensor)
+    altob_status iteration(int nk, double eps, int max_iters, cudaStream_t st)
+    {
+        for (int j = 0; j < maxN; ++j) {
+            const int n = nlist[j];
+            if (!n) continue;
+            const int* L = d_list[j];
+            k_b_zero<FT><<<dim3(gx_elem, n), 256, 0, st>>>(d_desc, L, d_active, j);
+            for (auto& c : classes) ALTOB_TRY(mttkrp_class(*c, j, st));
+            k_b_copym<FT><<<dim3(gx_elem, n), 256, 0, st>>>(d_desc, L, d_active, j);
+            k_b_prep<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, j, nk);
+            k_b_solve<FT><<<n, DN_THREADS, smem_solve(), st>>>(d_desc, L, d_active, j);
+            k_b_apply<FT><<<dim3(gx_apply, n), DN_THREADS, smem_apply(), st>>>(d_desc, L, d_active, j, nk);
+            k_b_lambda<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, nk);
+            k_b_gram<FT><<<dim3(gx_apply, n), DN_THREADS, smem_gram(), st>>>(d_desc, L, d_active, j, 1);
+            ALTOB_LAUNCH_CHECK();
+        }
+        k_b_fit<FT><<<count, DN_THREADS, 0, st>>>(d_desc, d_active, d_iters, eps, max_iters);
+        ALTOB_LAUNCH_CHECK();
+        return ALTOB_OK;
+    }
+
+    altob_status capture(double eps, int max_iters)
+    {
+        drop_graph();
+        if (!cap_stream) ALTOB_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        ALTOB_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+        altob_status s = iteration(NORM_MAX, eps, max_iters, cap_stream);
+        cudaError_t e = cudaStreamEndCapture(cap_stream, &g);
+        if (s != ALTOB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            gexec = nullptr;
+            return fail(ALTOB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        g_eps = eps;
+        g_iters = max_iters;
+        return ALTOB_OK;
+    }
+
+    altob_status any_active(cudaStream_t st, bool* any)
+    {
+        std::vector<int> a(count);
+        ALTOB_CUDA(cudaMemcpyAsync(a.data(), d_active, count * sizeof(int), cudaMemcpyDeviceToHost, st));
+        ALTOB_CUDA(cudaStreamSynchronize(st));
+        *any = std::any_of(a.begin(), a.end(), [](int v) { return v != 0; });
+        return ALTOB_OK;
+    }
+
+    altob_status solve(int max_iters, double eps, double* fits, int* iters, int use_graph, cudaStream_t st) override
+    {
+        if (max_iters < 1 || max_iters > cap) return fail(ALTOB_ERR_ARG, "max_iters must be 1..fit capacity");
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_solve<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve()));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_apply<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_apply()));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_gram<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_gram()));
+        // all tensors active, no fits yet; Grams of the initial factors
+        std::vector<int> ones(count, 1);
+        ALTOB_CUDA(cudaMemcpyAsync(d_active, ones.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+        ALTOB_CUDA(cudaMemsetAsync(d_iters, 0, count * sizeof(int), st));
+        for (int j = 0; j < maxN; ++j) {
+            if (!nlist[j]) continue;
+            k_b_prep<FT><<<nlist[j], 128, 0, st>>>(d_desc, d_list[j], d_active, j, NORM_2);
+            k_b_gram<FT><<<dim3(gx_apply, nlist[j]), DN_THREADS, smem_gram(), st>>>(d_desc, d_list[j], d_active, j, 0);
+        }
+        ALTOB_LAUNCH_CHECK();
+        // the first iteration normalises with the 2-norm, later ones with the max-norm
+        ALTOB_TRY(iteration(NORM_2, eps, max_iters, st));
+        int done = 1;
+        constexpr int CHUNK = 4;  // iterations between host checks for early exit
+        if (use_graph && max_iters > 1 && (!gexec || g_eps != eps || g_iters != max_iters))
+            ALTOB_TRY(capture(eps, max_iters));
+        while (done < max_iters) {
+            const int n = std::min(CHUNK, max_iters - done);
+            for (int i = 0; i < n; ++i) {
+                if (use_graph) ALTOB_CUDA(cudaGraphLaunch(gexec, st));
+                else ALTOB_TRY(iteration(NORM_MAX, eps, max_iters, st));
+            }
+            done += n;
+            if (done < max_iters) {
+                bool any = true;
+                ALTOB_TRY(any_active(st, &any));
+                if (!any) break;
+            }
+        }
+        k_b_lamout<FT><<<count, 128, 0, st>>>(d_desc, count);
+        ALTOB_LAUNCH_CHECK();
+        std::vector<int> hit(count);
+        ALTOB_CUDA(cudaMemcpyAsync(hit.data(), d_iters, count * sizeof(int), cudaMemcpyDeviceToHost, st));
+        std::vector<double> hf((size_t)count * cap);
+        ALTOB_CUDA(cudaMemcpyAsync(hf.data(), hdesc[0].fits, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        ALTOB_CUDA(cudaStreamSynchronize(st));
+        for (int b = 0; b < count; ++b) {
+            if (iters) iters[b] = hit[b];
+            if (fits)
+                for (int i = 0; i < max_iters; ++i)
+                    fits[(size_t)b * max_iters + i] = i < hit[b] ? hf[(size_t)b * cap + i] : 0.0;
+        }
+        return ALTOB_OK;
+    }
+
+    // Autotuner: per shape class, times each candidate (slot count x lane
+    // layout) on the class's MTTKRP of every mode and keeps the fastest.  The
+    // target factors are saved before and restored after, so the model the
+    // caller passed in is unchanged.
+    altob_status autotune(cudaStream_t st) override
+    {
+        drop_graph();
+        std::vector<int> ones(count, 1);
+        ALTOB_CUDA(cudaMemcpyAsync(d_active, ones.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ALTOB_CUDA(cudaEventCreate(&e0));
+        ALTOB_CUDA(cudaEventCreate(&e1));
+        altob_status s = ALTOB_OK;
+        for (auto& cp : classes) {
+            ClassRun<FT>& c = *cp;
+            // save the factors this class writes
+            size_t bytes = 0;
+            for (int b : c.members)
+                for (int m = 0; m < ts[b]->nmode; ++m) bytes += ts[b]->dims[m] * hdesc[b].R * sizeof(FT);
+            void* save = nullptr;
+            s = dmalloc(&save, bytes);
+            if (s != ALTOB_OK) break;
+            size_t off = 0;
+            for (int b : c.members)
+                for (int m = 0; m < ts[b]->nmode; ++m) {
+                    const size_t nb = ts[b]->dims[m] * hdesc[b].R * sizeof(FT);
+                    cudaMemcpyAsync((char*)save + off, hdesc[b].U[m], nb, cudaMemcpyDeviceToDevice, st);
+                    off += nb;
+                }
+            struct Cand {
+                int hs, lpn, ch;
+            };
+            std::vector<Cand> cand;
+            const int lpn0 = c.lpn, ch0 = c.ch;
+            for (int hs : {0, 512, 1024, 2048, 4096}) {
+                cand.push_back({hs, lpn0, ch0});
+                if (ch0 == 1 && c.vec > 1 && lpn0 >= 8) cand.push_back({hs, lpn0 / 2, 2});
+            }
+            Cand best = {c.hslots, lpn0, ch0};
+            float best_ms = 1e30f;
+            for (const Cand& k : cand) {
+                if (set_choice(c, k.hs, k.lpn, k.ch, st) != ALTOB_OK) continue;
+                float t_best = 1e30f;
+                bool ok = true;
+                for (int rep = 0; rep < 3 && ok; ++rep) {
+                    cudaEventRecord(e0, st);
+                    for (int j = 0; j < maxN && ok; ++j) ok = mttkrp_class(c, j, st) == ALTOB_OK;
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) ok = false;
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (rep > 0) t_best = std::min(t_best, ms);  // first run warms up
+                }
+                if (ok && t_best < best_ms) {
+                    best_ms = t_best;
+                    best = k;
+                }
+            }
+            off = 0;
+            for (int b : c.members)
+                for (int m = 0; m < ts[b]->nmode; ++m) {
+                    const size_t nb = ts[b]->dims[m] * hdesc[b].R * sizeof(FT);
+                    cudaMemcpyAsync(hdesc[b].U[m], (char*)save + off, nb, cudaMemcpyDeviceToDevice, st);
+                    off += nb;
+                }
+            dfree(save);
+            s = set_choice(c, best.hs, best.lpn, best.ch, st);
+            if (s != ALTOB_OK) break;
+            c.tuned_ms = best_ms;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ALTOB_CUDA(cudaGetLastError());
+        ALTOB_CUDA(cudaStreamSynchronize(st));
+        return s;
+    }
+
+    void describe(std::string* out) const override
+    {
+        char line[320];
+        snprintf(line, sizeof(line), "tensors=%d classes=%zu max_modes=%d max_rank=%d\n", count, classes.size(),
+                 maxN, maxR);
+        *out += line;
+        for (auto& c : classes) {
+            snprintf(line, sizeof(line), "class %s: tensors=%zu slots=%d lanes=%d chunks=%d tuned_ms=%.4f\n",
+                     c->key.c_str(), c->members.size(), c->hslots, c->lpn, c->ch, c->tuned_ms);
+            *out += line;
+        }
+    }
+
+    altob_status create(altob_tensor* const* tensors, int n, const uint64_t* ranks, void* const* const* dU,
+                        void* const* dlam, int fit_cap, cudaStream_t st)
+    {
+        count = n;
+        cap = fit_cap;
+        ts.assign(tensors, tensors + n);
+        hdesc.resize(n);
+        // per-tensor FP64 block (Grams, W, colacc, lambda, inner, fit) and the
+        // saved MTTKRP of the last mode, then the fit history and info
+        auto dbl_block = [](int N, int R) {
+            const size_t nd = (size_t)N * R * R + (size_t)R * R + 3 * (size_t)R + 2;
+            return (nd * 8 + 255) & ~(size_t)255;
+        };
+        size_t total = 0;
+        std::vector<size_t> off(n);
+        for (int b = 0; b < n; ++b) {
+            altob_tensor* t = ts[b];
+            const int R = (int)ranks[b];
+            maxN = std::max(maxN, t->nmode);
+            maxR = std::max(maxR, R);
+            off[b] = total;
+            total += dbl_block(t->nmode, R);
+            total += (t->dims[t->nmode - 1] * R * sizeof(FT) + 255) & ~(size_t)255;
+        }
+        const size_t fits_off = total;
+        total += ((size_t)n * cap * 8 + 255) & ~(size_t)255;
+        const size_t info_off = total;
+        total += 256;
+        ALTOB_TRY(dmalloc(&d_scratch, total));
+        char* base = (char*)d_scratch;
+        ALTOB_CUDA(cudaMemsetAsync(base + info_off, 0, 256, st));
+        std::vector<const void*> hv(n);
+        std::vector<u64> hnnz(n);
+        for (int b = 0; b < n; ++b) {
+            altob_tensor* t = ts[b];
+            BDesc<FT>& d = hdesc[b];
+            memset(&d, 0, sizeof(d));
+            const int R = (int)ranks[b];
+            d.nmode = t->nmode;
+            d.R = R;
+            for (int m = 0; m < t->nmode; ++m) {
+                d.U[m] = (FT*)dU[b][m];
+                d.dims[m] = t->dims[m];
+            }
+            double* p = (double*)(base + off[b]);
+            d.G = p;
+            p += (size_t)t->nmode * R * R;
+            d.W = p;
+            p += (size_t)R * R;
+            d.colacc = p;
+            p += R;
+            d.lam = p;
+            p += R;
+            d.inner = p;
+            p += R;
+            d.fit_tmp = p;
+            d.M = (FT*)(base + off[b] + dbl_block(t->nmode, R));
+            d.fits = (double*)(base + fits_off) + (size_t)b * cap;
+            d.lam_out = dlam ? (FT*)dlam[b] : nullptr;
+            d.normAT = 0.0;
+            d.info = (int*)(base + info_off);
+            hv[b] = t->d_vals;
+            hnnz[b] = t->nnz;
+        }
+        ALTOB_TRY(dmalloc_t(&d_desc, n));
+        ALTOB_TRY(dmalloc_t(&d_active, n));
+        ALTOB_TRY(dmalloc_t(&d_iters, n));
+        ALTOB_CUDA(cudaMemcpyAsync(d_desc, hdesc.data(), n * sizeof(BDesc<FT>), cudaMemcpyHostToDevice, st));
+        // squared norm of every tensor's values (cpd.hpp:73-79)
+        {
+            const void** d_vals = nullptr;
+            u64* d_nnz = nullptr;
+            ALTOB_TRY(dmalloc_t(&d_vals, n));
+            ALTOB_TRY(dmalloc_t(&d_nnz, n));
+            ALTOB_CUDA(cudaMemcpyAsync(d_vals, hv.data(), n * sizeof(void*), cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(d_nnz, hnnz.data(), n * sizeof(u64), cudaMemcpyHostToDevice, st));
+            if (ts[0]->vdt == ALTOB_U32)
+                k_b_sumsq<FT, u32><<<dim3(64, n), 256, 0, st>>>(d_desc, (const void* const*)d_vals, d_nnz);
+            else
+                k_b_sumsq<FT, FT><<<dim3(64, n), 256, 0, st>>>(d_desc, (const void* const*)d_vals, d_nnz);
+            ALTOB_LAUNCH_CHECK();
+            ALTOB_CUDA(cudaStreamSynchronize(st));
+            dfree((void*)d_vals);
+            dfree(d_nnz);
+        }
+        // per-mode lists of the tensors that have that mode
+        u64 maxrows = 1;
+        for (int j = 0; j < maxN; ++j) {
+            std::vector<int> L;
+            for (int b = 0; b < n; ++b)
+                if (ts[b]->nmode > j) {
+                    L.push_back(b);
+                    maxrows = std::max<u64>(maxrows, ts[b]->dims[j]);
+                }
+            nlist[j] = (int)L.size();
+            if (L.empty()) continue;
+            ALTOB_TRY(dmalloc_t(&d_list[j], L.size()));
+            ALTOB_CUDA(cudaMemcpyAsync(d_list[j], L.data(), L.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        }
+        gx_apply = (int)std::max<u64>(1, std::min<u64>(64, (maxrows + 255) / 256));
+        gx_elem = (int)std::max<u64>(1, std::min<u64>(64, (maxrows * maxR + 4095) / 4096));
+        // shape classes: (order 3 | 4-5, lanes, elements per lane, chunks)
+        std::map<std::string, ClassRun<FT>*> byk;
+        for (int b = 0; b < n; ++b) {
+            altob_tensor* t = ts[b];
+            bool aligned = true;
+            for (int m = 0; m < t->nmode; ++m) aligned = aligned && ptr_aligned16(hdesc[b].U[m]);
+            TiledPlan pl;
+            ALTOB_TRY(plan_tiled(t, (u64)hdesc[b].R, sizeof(FT), aligned, true, &pl));
+            const int nm = t->nmode == 3 ? 3 : 0;
+            char k[128];
+            snprintf(k, sizeof(k), "order=%s lanes=%d vec=%d chunks=%d", nm == 3 ? "3" : "4-5", pl.lpn, pl.vec,
+                     pl.ch);
+            auto it = byk.find(k);
+            if (it == byk.end()) {
+                auto c = std::make_unique<ClassRun<FT>>();
+                c->nm = nm;
+                c->vdt = t->vdt;
+                c->key = k;
+                c->lpn = pl.lpn;
+                c->vec = pl.vec;
+                c->ch = pl.ch;
+                c->hslots = 2048;
+                it = byk.emplace(k, c.get()).first;
+                classes.push_back(std::move(c));
+            }
+            it->second->members.push_back(b);
+        }
+        for (auto& c : classes) ALTOB_TRY(set_choice(*c, c->hslots, c->lpn, c->ch, st));
+        ALTOB_CUDA(cudaStreamSynchronize(st));
+        return ALTOB_OK;
+    }
+};
+
+}  // namespace altob
+
+struct altob_batch {
+    std::unique_ptr<altob::BatchBase> impl;
+};
+
+using namespace altob;
+
+extern "C" {
+
+altob_status altob_batch_create(altob_tensor* const* tensors, int count, const uint64_t* ranks, altob_dtype ftype,
+                                void* const* const* d_factors, void* const* d_lambda, int fit_capacity, void* stream,
+                                altob_batch** out)
+{
+    if (!out) return fail(ALTOB_ERR_ARG, "NULL output handle");
+    *out = nullptr;
+    if (!tensors || !ranks || !d_factors || count < 1) return fail(ALTOB_ERR_ARG, "NULL or empty argument");
+    if (count > 65535) return fail(ALTOB_ERR_UNSUPPORTED, "more than 65535 tensors in one batch");
+    if (ftype != ALTOB_F64 && ftype != ALTOB_F32) return fail(ALTOB_ERR_ARG, "dtype must be F64 or F32");
+    if (fit_capacity < 1) return fail(ALTOB_ERR_ARG, "fit capacity must be >= 1");
+    for (int b = 0; b < count; ++b) {
+        altob_tensor* t = tensors[b];
+        if (!t || !d_factors[b]) return fail(ALTOB_ERR_ARG, "NULL tensor or factor list");
+        ALTOB_TRY(check_model(t, ftype, d_factors[b], ranks[b]));
+        if (t->nmode < 2) return fail(ALTOB_ERR_ARG, "CP-ALS needs at least two modes");
+        if (t->nnz == 0) return fail(ALTOB_ERR_ARG, "CP-ALS on an empty tensor (the fit divides by its norm)");
+        if (t->vdt != tensors[0]->vdt) return fail(ALTOB_ERR_ARG, "all tensors of a batch need one value dtype");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
+    std::unique_ptr<altob_batch> bh(new altob_batch());
+    altob_status s;
+    if (ftype == ALTOB_F64) {
+        auto* impl = new BatchImpl<double>();
+        bh->impl.reset(impl);
+        s = impl->create(tensors, count, ranks, d_factors, d_lambda, fit_capacity, st);
+    } else {
+        auto* impl = new BatchImpl<float>();
+        bh->impl.reset(impl);
+        s = impl->create(tensors, count, ranks, d_factors, d_lambda, fit_capacity, st);
+    }
+    if (s != ALTOB_OK) return s;
+    *out = bh.release();
+    return ALTOB_OK;
+}
+
+altob_status altob_batch_autotune(altob_batch* b, void* stream)
+{
+    if (!b) return fail(ALTOB_ERR_ARG, "NULL batch");
+    StreamScope scope((cudaStream_t)stream);
+    return b->impl->autotune((cudaStream_t)stream);
+}
+
+altob_status altob_batch_cpd_als(altob_batch* b, int max_iters, double epsilon, double* fits, int* iters,
+                                 int use_graph, void* stream)
+{
+    if (!b) return fail(ALTOB_ERR_ARG, "NULL batch");
+    StreamScope scope((cudaStream_t)stream);
+    return b->impl->solve(max_iters, epsilon, fits, iters, use_graph, (cudaStream_t)stream);
+}
+
+altob_status altob_batch_describe(const altob_batch* b, char* buf, size_t len)
+{
+    if (!b || !buf || !len) return fail(ALTOB_ERR_ARG, "NULL argument");
+    std::string s;
+    b->impl->describe(&s);
+    const size_t n = std::min(len - 1, s.size());
+    memcpy(buf, s.data(), n);
+    buf[n] = 0;
+    return ALTOB_OK;
+}
+
+altob_status altob_batch_destroy(altob_batch* b)
+{
+    if (!b) return ALTOB_OK;
+    ALTOB_CUDA(cudaDeviceSynchronize());
+    delete b;
+    return ALTOB_OK;
+}
+
+}  // extern "C"

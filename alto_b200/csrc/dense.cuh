@@ -19,6 +19,9 @@ constexpr int SOLVE_MAX_RANK = 112;  // two R x R FP64 matrices in shared memory
 
 enum NormKind { NORM_NONE = 0, NORM_2 = 1, NORM_MAX = 2 };
 
+// Argument checks shared by the CP-ALS / CP-APR entry points (cpd.cu).
+altob_status check_model(const altob_tensor* t, altob_dtype ft, void* const* dU, u64 rank);
+
 // Host launchers (dense.cu).  All FP64 internally; FT = storage type.
 template <typename FT>
 altob_status gram(const FT* U, u64 I, int R, double* G, const double* div, FT* Uout, const FT* M,

@@ -539,8 +539,51 @@ __device__ __forceinline__ void run_add(FT (*racc)[VEC], FT (*x)[VEC])
     }
 }
 
+// Shared-memory work areas of the grouped kernels (tags and counts must be
+// zero between tiles; grouped_tile leaves them zero).
+struct GroupedSmem {
+    u32* rec;
+    u32* srec;
+    u32* tag;
+    u32* cnt;
+    u32* used;
+    u32* nused;
+    u32* ndirect;
+    u32* wsum;
+};
+
+template <typename FT, int MM>
+__device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, int H, u32* statics)
+{
+    constexpr int RW = RecWords<FT, MM>::n;
+    GroupedSmem g;
+    g.rec = reinterpret_cast<u32*>(smem);
+    g.srec = g.rec + (size_t)GT_TILE * RW;
+    g.tag = g.srec + (size_t)GT_TILE * RW;
+    g.cnt = g.tag + H;
+    g.used = g.cnt + H;
+    g.nused = statics;
+    g.ndirect = statics + 1;
+    g.wsum = statics + 2;
+    return g;
+}
+
+__device__ __forceinline__ void grouped_init(const GroupedSmem& g, int H)
+{
+    for (int k = threadIdx.x; k < H; k += MT_THREADS) {
+        g.tag[k] = 0;
+        g.cnt[k] = 0;
+    }
+    if (threadIdx.x == 0) {
+        *g.nused = 0;
+        *g.ndirect = 0;
+    }
+    __syncthreads();
+}
+
+// One tile of nonzeros [ti * GT_TILE, ...) of the tensor described by `a`.
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
+__device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, const GroupedSmem& gs)
 {
     constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
     constexpr int NPW = 32 / LPN;
@@ -548,27 +591,18 @@ __global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
     constexpr int NGRP = MT_WARPS * NPW;
     constexpr int IPG = GT_TILE / NGRP;  // sorted nonzeros per lane group
     constexpr int FW = (int)(sizeof(FT) / 4);
-    extern __shared__ __align__(16) unsigned char smem[];
     const int R = a.R, H = a.hslots;
     const int nmode = NM ? NM : a.nmode;
-    u32* rec = reinterpret_cast<u32*>(smem);
-    u32* srec = rec + (size_t)GT_TILE * RW;  // records in run order
-    u32* tag = srec + (size_t)GT_TILE * RW;
-    u32* cnt = tag + H;
-    u32* used = cnt + H;
-    __shared__ u32 nused, ndirect, wsum[MT_WARPS];
+    u32* rec = gs.rec;
+    u32* srec = gs.srec;
+    u32* tag = gs.tag;
+    u32* cnt = gs.cnt;
+    u32* used = gs.used;
+    u32& nused = *gs.nused;
+    u32& ndirect = *gs.ndirect;
+    u32* wsum = gs.wsum;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int k = tid; k < H; k += MT_THREADS) {
-        tag[k] = 0;
-        cnt[k] = 0;
-    }
-    if (tid == 0) {
-        nused = 0;
-        ndirect = 0;
-    }
-    __syncthreads();
-
     const VT* vals = reinterpret_cast<const VT*>(a.vals);
     const int target = a.target;
     const int sub = lane % LPN, q = lane / LPN;
@@ -580,222 +614,265 @@ __global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
     for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : (k + 1 < MM ? k + 1 : k)];
     const FT* Ut = a.U[target];
     const int nother = nmode - 1;
-
-    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) {
-        const u64 g0 = ti * (u64)GT_TILE;
-        const int nvalid = (int)min((u64)GT_TILE, a.nnz - g0);
-        u64 hcur = 0, hnext = 0, nstart = ~0ull;
-        bool slow_hi = a.perm != nullptr;
-        if (!a.key.khi && a.key.nrun && !slow_hi) {
-            const int r = run_of(a.key, g0);
-            hcur = a.key.run_val[r];
-            if (r + 1 < a.key.nrun) {
-                nstart = a.key.run_start[r + 1];
-                hnext = a.key.run_val[r + 1];
-                if (r + 2 < a.key.nrun && a.key.run_start[r + 2] < g0 + (u64)GT_TILE) slow_hi = true;
+    const u64 g0 = ti * (u64)GT_TILE;
+    const int nvalid = (int)min((u64)GT_TILE, a.nnz - g0);
+    u64 hcur = 0, hnext = 0, nstart = ~0ull;
+    bool slow_hi = a.perm != nullptr;
+    if (!a.key.khi && a.key.nrun && !slow_hi) {
+        const int r = run_of(a.key, g0);
+        hcur = a.key.run_val[r];
+        if (r + 1 < a.key.nrun) {
+            nstart = a.key.run_start[r + 1];
+            hnext = a.key.run_val[r + 1];
+            if (r + 2 < a.key.nrun && a.key.run_start[r + 2] < g0 + (u64)GT_TILE) slow_hi = true;
+        }
+    }
+    // ---- A1: records [target, others..., value], slot claims, ranks
+    u64 lo[GT_IPT], posv[GT_IPT];
+    VT vv[GT_IPT];
+#pragma unroll
+    for (int k = 0; k < GT_IPT; ++k) {
+        const int it = tid + k * MT_THREADS;
+        const u64 g = g0 + it;
+        posv[k] = 0;
+        if (it < nvalid) {
+            const u64 pos = a.perm ? (u64)a.perm[g] : g;
+            posv[k] = pos;
+            lo[k] = a.key.klo[pos];
+            vv[k] = vals[pos];
+        }
+    }
+    int slv[GT_IPT];
+    u32 rankv[GT_IPT];
+#pragma unroll
+    for (int k = 0; k < GT_IPT; ++k) {
+        const int it = tid + k * MT_THREADS;
+        const u64 g = g0 + it;
+        int sl = -2;
+        bool claimed = false;
+        u32 h = 0;
+        if (it < nvalid) {
+            u64 hi;
+            if (a.key.khi) hi = a.key.khi[posv[k]];
+            else if (a.key.nrun == 0) hi = 0;
+            else if (slow_hi) hi = key_hi(a.key, posv[k]);
+            else hi = g >= nstart ? hnext : hcur;
+            u32* r = rec + (size_t)it * RW;
+            u32 trow = 0;
+#pragma unroll
+            for (int m = 0; m < MM; ++m) {
+                if (NM == 0 && m >= nmode) break;
+                const u32 c = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
+                r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
+                if (m == target) trow = c;
+            }
+            const FT fv = (FT)vv[k];
+            if constexpr (FW == 1) {
+                r[MM] = __float_as_uint((float)fv);
+            } else {
+                const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
+                r[MM] = (u32)b;
+                r[MM + 1] = (u32)(b >> 32);
+            }
+            sl = -1;
+            if (H) {
+                h = trow & (u32)(H - 1);
+                const u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
+                if (old == 0u) {
+                    claimed = true;
+                    sl = (int)h;
+                } else if (old == trow + 1u) {
+                    sl = (int)h;
+                }
             }
         }
-        // ---- A1: records [target, others..., value], slot claims, ranks
-        u64 lo[GT_IPT], posv[GT_IPT];
-        VT vv[GT_IPT];
-#pragma unroll
-        for (int k = 0; k < GT_IPT; ++k) {
-            const int it = tid + k * MT_THREADS;
-            const u64 g = g0 + it;
-            posv[k] = 0;
-            if (it < nvalid) {
-                const u64 pos = a.perm ? (u64)a.perm[g] : g;
-                posv[k] = pos;
-                lo[k] = a.key.klo[pos];
-                vv[k] = vals[pos];
-            }
-        }
-        int slv[GT_IPT];
-        u32 rankv[GT_IPT];
-#pragma unroll
-        for (int k = 0; k < GT_IPT; ++k) {
-            const int it = tid + k * MT_THREADS;
-            const u64 g = g0 + it;
-            int sl = -2;
-            bool claimed = false;
-            u32 h = 0;
-            if (it < nvalid) {
-                u64 hi;
-                if (a.key.khi) hi = a.key.khi[posv[k]];
-                else if (a.key.nrun == 0) hi = 0;
-                else if (slow_hi) hi = key_hi(a.key, posv[k]);
-                else hi = g >= nstart ? hnext : hcur;
-                u32* r = rec + (size_t)it * RW;
-                u32 trow = 0;
-#pragma unroll
-                for (int m = 0; m < MM; ++m) {
-                    if (NM == 0 && m >= nmode) break;
-                    const u32 c = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
-                    r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
-                    if (m == target) trow = c;
-                }
-                const FT fv = (FT)vv[k];
-                if constexpr (FW == 1) {
-                    r[MM] = __float_as_uint((float)fv);
-                } else {
-                    const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
-                    r[MM] = (u32)b;
-                    r[MM + 1] = (u32)(b >> 32);
-                }
-                sl = -1;
-                if (H) {
-                    h = trow & (u32)(H - 1);
-                    const u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
-                    if (old == 0u) {
-                        claimed = true;
-                        sl = (int)h;
-                    } else if (old == trow + 1u) {
-                        sl = (int)h;
-                    }
-                }
-            }
-            const u32 cm = __ballot_sync(0xffffffffu, claimed);
-            if (cm) {
-                u32 base = 0;
-                if (lane == 0) base = atomicAdd(&nused, (u32)__popc(cm));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (claimed) used[base + __popc(cm & lt_mask)] = h;
-            }
-            const u32 key = sl >= 0 ? (u32)sl : (0x80000000u | (u32)lane);
-            const u32 peers = __match_any_sync(0xffffffffu, key);
-            const int leader = __ffs(peers) - 1;
+        const u32 cm = __ballot_sync(0xffffffffu, claimed);
+        if (cm) {
             u32 base = 0;
-            if (sl >= 0 && lane == leader) base = atomicAdd(&cnt[sl], (u32)__popc(peers));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            u32 rank = base + __popc(peers & lt_mask);
-            const u32 dm = __ballot_sync(0xffffffffu, sl == -1);
-            if (dm) {
-                u32 db = 0;
-                if (lane == 0) db = atomicAdd(&ndirect, (u32)__popc(dm));
-                db = __shfl_sync(0xffffffffu, db, 0);
-                if (sl == -1) rank = db + __popc(dm & lt_mask);
-            }
-            slv[k] = sl;
-            rankv[k] = rank;
+            if (lane == 0) base = atomicAdd(&nused, (u32)__popc(cm));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (claimed) used[base + __popc(cm & lt_mask)] = h;
         }
-        __syncthreads();
-        // ---- A2: exclusive scan of the counts in claim order
-        const u32 nu = nused;
-        {
-            u32 c[GT_IPT], sum = 0;
-#pragma unroll
-            for (int k = 0; k < GT_IPT; ++k) {
-                const u32 e = (u32)(tid * GT_IPT + k);
-                c[k] = e < nu ? cnt[used[e]] : 0u;
-                sum += c[k];
-            }
-            u32 xs = sum;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const u32 y = __shfl_up_sync(0xffffffffu, xs, o);
-                if (lane >= o) xs += y;
-            }
-            if (lane == 31) wsum[warp] = xs;
-            __syncthreads();
-            u32 wbase = 0;
-#pragma unroll
-            for (int w = 0; w < MT_WARPS; ++w)
-                if (w < warp) wbase += wsum[w];
-            u32 run = wbase + xs - sum;
-#pragma unroll
-            for (int k = 0; k < GT_IPT; ++k) {
-                const u32 e = (u32)(tid * GT_IPT + k);
-                if (e < nu) {
-                    const u32 hh = used[e];
-                    tag[hh] = 0;    // tags are not read again in this tile
-                    cnt[hh] = run;  // count -> start offset
-                }
-                run += c[k];
-            }
+        const u32 key = sl >= 0 ? (u32)sl : (0x80000000u | (u32)lane);
+        const u32 peers = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(peers) - 1;
+        u32 base = 0;
+        if (sl >= 0 && lane == leader) base = atomicAdd(&cnt[sl], (u32)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        u32 rank = base + __popc(peers & lt_mask);
+        const u32 dm = __ballot_sync(0xffffffffu, sl == -1);
+        if (dm) {
+            u32 db = 0;
+            if (lane == 0) db = atomicAdd(&ndirect, (u32)__popc(dm));
+            db = __shfl_sync(0xffffffffu, db, 0);
+            if (sl == -1) rank = db + __popc(dm & lt_mask);
         }
-        __syncthreads();
-        // ---- A3: records into run order (counting-sort scatter)
-        u32 slotted = 0;
-#pragma unroll
-        for (int w = 0; w < MT_WARPS; ++w) slotted += wsum[w];
+        slv[k] = sl;
+        rankv[k] = rank;
+    }
+    __syncthreads();
+    // ---- A2: exclusive scan of the counts in claim order
+    const u32 nu = nused;
+    {
+        u32 c[GT_IPT], sum = 0;
 #pragma unroll
         for (int k = 0; k < GT_IPT; ++k) {
-            const int it = tid + k * MT_THREADS;
-            if (it < nvalid) {
-                const int sl = slv[k];
-                const u32 pos = sl >= 0 ? cnt[sl] + rankv[k] : slotted + rankv[k];
-                const u32* src = rec + (size_t)it * RW;
-                u32* dst = srec + (size_t)pos * RW;
-#pragma unroll
-                for (int w4 = 0; w4 < RW; w4 += 4)
-                    *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
-            }
+            const u32 e = (u32)(tid * GT_IPT + k);
+            c[k] = e < nu ? cnt[used[e]] : 0u;
+            sum += c[k];
         }
+        u32 xs = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(0xffffffffu, xs, o);
+            if (lane >= o) xs += y;
+        }
+        if (lane == 31) wsum[warp] = xs;
         __syncthreads();
-        // ---- B: runs of equal output rows, one atomic per run
-        u32 prow = 0xffffffffu;
-        FT racc[CH][VEC];
+        u32 wbase = 0;
 #pragma unroll
-        for (int ch = 0; ch < CH; ++ch)
+        for (int w = 0; w < MT_WARPS; ++w)
+            if (w < warp) wbase += wsum[w];
+        u32 run = wbase + xs - sum;
 #pragma unroll
-            for (int e = 0; e < VEC; ++e) racc[ch][e] = FT(0);
-        const int p0 = grp * IPG;
-        const int pend = min(p0 + IPG, nvalid);
-        int p = p0;
-        // two nonzeros per step: both gathers in flight before the run logic
-        for (; p + 1 < pend; p += 2) {
-            u32 w0[RW], w1[RW];
-            load_rec<FT, RW>(srec + (size_t)p * RW, w0);
-            load_rec<FT, RW>(srec + (size_t)(p + 1) * RW, w1);
-            FT x0[CH][VEC], x1[CH][VEC];
-            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
-            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w1, Uo, Ut, R, sub, nother, a.eps, gmask, x1);
-            if (w0[0] != prow) {
-                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-                prow = w0[0];
-#pragma unroll
-                for (int ch = 0; ch < CH; ++ch)
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
-            } else {
-                run_add<FT, VEC, CH>(racc, x0);
+        for (int k = 0; k < GT_IPT; ++k) {
+            const u32 e = (u32)(tid * GT_IPT + k);
+            if (e < nu) {
+                const u32 hh = used[e];
+                tag[hh] = 0;    // tags are not read again in this tile
+                cnt[hh] = run;  // count -> start offset
             }
-            if (w1[0] != prow) {
-                flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-                prow = w1[0];
-#pragma unroll
-                for (int ch = 0; ch < CH; ++ch)
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x1[ch][e];
-            } else {
-                run_add<FT, VEC, CH>(racc, x1);
-            }
+            run += c[k];
         }
-        if (p < pend) {
-            u32 w0[RW];
-            load_rec<FT, RW>(srec + (size_t)p * RW, w0);
-            FT x0[CH][VEC];
-            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
-            if (w0[0] != prow) {
-                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-                prow = w0[0];
+    }
+    __syncthreads();
+    // ---- A3: records into run order (counting-sort scatter)
+    u32 slotted = 0;
 #pragma unroll
-                for (int ch = 0; ch < CH; ++ch)
+    for (int w = 0; w < MT_WARPS; ++w) slotted += wsum[w];
 #pragma unroll
-                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
-            } else {
-                run_add<FT, VEC, CH>(racc, x0);
-            }
+    for (int k = 0; k < GT_IPT; ++k) {
+        const int it = tid + k * MT_THREADS;
+        if (it < nvalid) {
+            const int sl = slv[k];
+            const u32 pos = sl >= 0 ? cnt[sl] + rankv[k] : slotted + rankv[k];
+            const u32* src = rec + (size_t)it * RW;
+            u32* dst = srec + (size_t)pos * RW;
+#pragma unroll
+            for (int w4 = 0; w4 < RW; w4 += 4)
+                *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
         }
-        if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-        __syncthreads();
-        // counts back to zero for the next tile (tags were cleared in A2)
-        for (u32 e = tid; e < nu; e += MT_THREADS) cnt[used[e]] = 0;
-        if (tid == 0) {
-            nused = 0;
-            ndirect = 0;
+    }
+    __syncthreads();
+    // ---- B: runs of equal output rows, one atomic per run
+    u32 prow = 0xffffffffu;
+    FT racc[CH][VEC];
+#pragma unroll
+    for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) racc[ch][e] = FT(0);
+    const int p0 = grp * IPG;
+    const int pend = min(p0 + IPG, nvalid);
+    int p = p0;
+    // two nonzeros per step: both gathers in flight before the run logic
+    for (; p + 1 < pend; p += 2) {
+        u32 w0[RW], w1[RW];
+        load_rec<FT, RW>(srec + (size_t)p * RW, w0);
+        load_rec<FT, RW>(srec + (size_t)(p + 1) * RW, w1);
+        FT x0[CH][VEC], x1[CH][VEC];
+        nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
+        nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w1, Uo, Ut, R, sub, nother, a.eps, gmask, x1);
+        if (w0[0] != prow) {
+            if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+            prow = w0[0];
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
+        } else {
+            run_add<FT, VEC, CH>(racc, x0);
         }
-        __syncthreads();
+        if (w1[0] != prow) {
+            flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+            prow = w1[0];
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) racc[ch][e] = x1[ch][e];
+        } else {
+            run_add<FT, VEC, CH>(racc, x1);
+        }
+    }
+    if (p < pend) {
+        u32 w0[RW];
+        load_rec<FT, RW>(srec + (size_t)p * RW, w0);
+        FT x0[CH][VEC];
+        nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
+        if (w0[0] != prow) {
+            if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+            prow = w0[0];
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
+        } else {
+            run_add<FT, VEC, CH>(racc, x0);
+        }
+    }
+    if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+    __syncthreads();
+    // counts back to zero for the next tile (tags were cleared in A2)
+    for (u32 e = tid; e < nu; e += MT_THREADS) cnt[used[e]] = 0;
+    if (tid == 0) {
+        nused = 0;
+        ndirect = 0;
+    }
+    __syncthreads();
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
+{
+    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 statics[2 + MT_WARPS];
+    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, a.hslots, statics);
+    grouped_init(gs, a.hslots);
+    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x)
+        grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(a, ti, gs);
+}
+
+// Batched form: the tiles of many tensors (one TiledArgs each, same shape
+// class and slot count) in one persistent launch.  tile_prefix[b] is the
+// first global tile of tensor b; tensors whose active flag is 0 are skipped.
+template <typename FT>
+struct BatchTiles {
+    const TiledArgs<FT>* args;
+    const u64* tile_prefix;  // ntensors + 1
+    const int* bid;          // batch index of each entry (for `active`)
+    const int* active;
+    int ntensors;
+    int hslots;
+    u64 total_tiles;
+};
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
+{
+    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 statics[2 + MT_WARPS];
+    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, bt.hslots, statics);
+    grouped_init(gs, bt.hslots);
+    for (u64 gt = blockIdx.x; gt < bt.total_tiles; gt += gridDim.x) {
+        int lo = 0, hi = bt.ntensors - 1;  // last tensor whose first tile <= gt
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bt.tile_prefix[mid] <= gt) lo = mid;
+            else hi = mid - 1;
+        }
+        if (!bt.active[bt.bid[lo]]) continue;
+        grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(bt.args[lo], gt - bt.tile_prefix[lo], gs);
     }
 }
 

@@ -22,6 +22,10 @@ altob_status launch_tiled(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
 template <typename FT, typename VT>
 altob_status launch_atomic_cr(const CrArgsK<FT>& a, cudaStream_t st);
 
+// Batched grouped MTTKRP over the tensors of one shape class (nm = 3 or 0).
+template <typename FT, typename VT>
+altob_status launch_batch(const BatchTiles<FT>& bt, int nm, const TiledCfg& c, cudaStream_t st, int* bps);
+
 // Sets the kernel's shared-memory limit once and launches it (or only
 // reports occupancy when grid.x == 0).
 template <typename K>
@@ -88,6 +92,37 @@ altob_status launch_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
     return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
 }
 
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH>
+altob_status launch_batch_one(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    static std::atomic<size_t> configured{0};
+    return launch_kernel(k_grouped_batch<FT, VT, NM, LPN, VEC, CH, false>, configured, &bt, c, st, bps);
+}
+
+template <typename FT, typename VT, int NM>
+altob_status launch_batch_shape(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    constexpr int V = 16 / sizeof(FT);
+    if (c.vec == 1) return launch_batch_one<FT, VT, NM, 32, 1, 4>(bt, c, st, bps);
+    if (c.ch == 2) {
+        switch (c.lpn) {
+        case 4: return launch_batch_one<FT, VT, NM, 4, V, 2>(bt, c, st, bps);
+        case 8: return launch_batch_one<FT, VT, NM, 8, V, 2>(bt, c, st, bps);
+        case 16: return launch_batch_one<FT, VT, NM, 16, V, 2>(bt, c, st, bps);
+        case 32: return launch_batch_one<FT, VT, NM, 32, V, 2>(bt, c, st, bps);
+        }
+        return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
+    }
+    switch (c.lpn) {
+    case 2: return launch_batch_one<FT, VT, NM, 2, V, 1>(bt, c, st, bps);
+    case 4: return launch_batch_one<FT, VT, NM, 4, V, 1>(bt, c, st, bps);
+    case 8: return launch_batch_one<FT, VT, NM, 8, V, 1>(bt, c, st, bps);
+    case 16: return launch_batch_one<FT, VT, NM, 16, V, 1>(bt, c, st, bps);
+    case 32: return launch_batch_one<FT, VT, NM, 32, V, 1>(bt, c, st, bps);
+    }
+    return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
+}
+
 #define ALTOB_INSTANTIATE_MTTKRP(FT, VT)                                                                 \
     template <>                                                                                        \
     altob_status launch_tiled<FT, VT>(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st,      \
@@ -97,6 +132,12 @@ altob_status launch_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
             return c.phi ? launch_shape<FT, VT, 3, true>(a, c, st, bps)                                \
                          : launch_shape<FT, VT, 3, false>(a, c, st, bps);                              \
         return c.phi ? launch_shape<FT, VT, 0, true>(a, c, st, bps) : launch_shape<FT, VT, 0, false>(a, c, st, bps); \
+    }                                                                                                  \
+    template <>                                                                                        \
+    altob_status launch_batch<FT, VT>(const BatchTiles<FT>& bt, int nm, const TiledCfg& c, cudaStream_t st, \
+                                      int* bps)                                                        \
+    {                                                                                                  \
+        return nm == 3 ? launch_batch_shape<FT, VT, 3>(bt, c, st, bps) : launch_batch_shape<FT, VT, 0>(bt, c, st, bps); \
     }                                                                                                  \
     template <>                                                                                        \
     altob_status launch_atomic_cr<FT, VT>(const CrArgsK<FT>& a, cudaStream_t st)                       \

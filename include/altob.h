@@ -225,6 +225,41 @@ ALTOB_API altob_status altob_loglik_noalloc(altob_tensor* t, altob_dtype ftype,
                                             double eps_div_zero,
                                             double* loglik, void* stream);
 
+/* ---- batched CP-ALS ----------------------------------------------------
+ * No counterpart in the reference (one tensor per run there).  Many
+ * independent CP-ALS solves (cpd_alto, include/cpd.hpp:43-186, each) run
+ * together: every step of an iteration (MTTKRP, R x R solve, row apply,
+ * normalisation, Gram, fit) is one launch for all tensors of the batch, the
+ * MTTKRP one launch per shape class, and iterations after the first are
+ * replayed from a captured CUDA graph.  Each tensor stops on its own rule
+ * (|fit - previous fit| < epsilon, or max_iters) and is skipped from then on,
+ * so its result is the one a separate altob_cpd_als call computes (up to the
+ * order of floating-point additions in the MTTKRP).
+ *   tensors[b], ranks[b] (1..112), d_factors[b][m] (device, dims[m] x
+ *   ranks[b], row-major, ftype) and d_lambda[b] (device, ranks[b]; the array
+ *   or any entry may be NULL) belong to tensor b.  All tensors share one
+ *   value dtype.  The handle keeps the pointers: factors are updated in place
+ *   by every altob_batch_cpd_als call.  fit_capacity bounds max_iters. */
+typedef struct altob_batch altob_batch;
+ALTOB_API altob_status altob_batch_create(altob_tensor* const* tensors, int count,
+                                          const uint64_t* ranks, altob_dtype ftype,
+                                          void* const* const* d_factors,
+                                          void* const* d_lambda, int fit_capacity,
+                                          void* stream, altob_batch** out);
+/* Picks, per shape class (order 3 or 4-5, lanes per nonzero, elements per
+ * lane), the row-slot count and lane layout of the batched MTTKRP by timing
+ * every candidate on that class; leaves the factors unchanged. */
+ALTOB_API altob_status altob_batch_autotune(altob_batch* b, void* stream);
+/* fits: count x max_iters (row b = tensor b, 0 after its last iteration) or
+ * NULL; iters: count or NULL.  use_graph = 0 launches every iteration
+ * directly (same results).  Synchronous on `stream`. */
+ALTOB_API altob_status altob_batch_cpd_als(altob_batch* b, int max_iters, double epsilon,
+                                           double* fits, int* iters, int use_graph,
+                                           void* stream);
+/* Text description of the shape classes and their chosen schedules. */
+ALTOB_API altob_status altob_batch_describe(const altob_batch* b, char* buf, size_t len);
+ALTOB_API altob_status altob_batch_destroy(altob_batch* b);
+
 /* ---- tensor files ------------------------------------------------------
  * Replaces ImportSparseTensor (sptensor.cpp:165-258).  The .tns reader
  * follows the reference (dims = largest index seen, '#' comments and empty
