@@ -41,29 +41,50 @@ struct BDesc {
 
 // ------------------------------------------------------------ kernels
 
-template <typename FT>
-__global__ void k_b_zero(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
-                         const int* __restrict__ active, int j)
+// Flattened per-mode grid: tensor list[i] owns blocks [prefix[i], prefix[i+1]),
+// so small tensors get few CTAs and large ones many.
+struct BlkMap {
+    const int* list;
+    const int* prefix;  // n + 1
+    int n;
+};
+
+__device__ __forceinline__ int blk_owner(const BlkMap& m, int* bx, int* nbx)
 {
-    const int b = list[blockIdx.y];
+    const int blk = (int)blockIdx.x;
+    int lo = 0, hi = m.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (m.prefix[mid] <= blk) lo = mid;
+        else hi = mid - 1;
+    }
+    *bx = blk - m.prefix[lo];
+    *nbx = m.prefix[lo + 1] - m.prefix[lo];
+    return m.list[lo];
+}
+
+template <typename FT>
+__global__ void k_b_zero(const BDesc<FT>* __restrict__ d, BlkMap map, const int* __restrict__ active, int j)
+{
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
     const u64 n = t.dims[j] * (u64)t.R;
     FT* U = t.U[j];
-    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x) U[e] = FT(0);
+    for (u64 e = (u64)bx * blockDim.x + threadIdx.x; e < n; e += (u64)nbx * blockDim.x) U[e] = FT(0);
 }
 
 template <typename FT>
-__global__ void k_b_copym(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
-                          const int* __restrict__ active, int j)
+__global__ void k_b_copym(const BDesc<FT>* __restrict__ d, BlkMap map, const int* __restrict__ active, int j)
 {
-    const int b = list[blockIdx.y];
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
     if (j != t.nmode - 1) return;
     const u64 n = t.dims[j] * (u64)t.R;
-    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (u64)gridDim.x * blockDim.x)
-        t.M[e] = t.U[j][e];
+    for (u64 e = (u64)bx * blockDim.x + threadIdx.x; e < n; e += (u64)nbx * blockDim.x) t.M[e] = t.U[j][e];
 }
 
 template <typename FT>
@@ -93,15 +114,15 @@ __global__ void __launch_bounds__(DN_THREADS) k_b_solve(const BDesc<FT>* __restr
     solve_body(t.G, t.nmode, j, t.R, t.W, t.info);
 }
 
-template <typename FT>
-__global__ void __launch_bounds__(DN_THREADS) k_b_apply(const BDesc<FT>* __restrict__ d,
-                                                        const int* __restrict__ list,
+template <typename FT, int LPR, int CJ>
+__global__ void __launch_bounds__(DN_THREADS) k_b_apply(const BDesc<FT>* __restrict__ d, BlkMap map,
                                                         const int* __restrict__ active, int j, int nk)
 {
-    const int b = list[blockIdx.y];
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
-    apply_body<FT>(t.U[j], t.dims[j], t.R, t.W, nk, t.colacc, blockIdx.x, gridDim.x);
+    apply_body<FT, LPR, CJ>(t.U[j], t.dims[j], t.R, t.W, nk, t.colacc, bx, nbx);
 }
 
 template <typename FT>
@@ -116,18 +137,18 @@ __global__ void k_b_lambda(const BDesc<FT>* __restrict__ d, const int* __restric
 
 // Gram of U_j; with `scaled`, U_j /= lambda first (written back) and the
 // fit's inner product with the saved MTTKRP of the last mode.
-template <typename FT>
-__global__ void __launch_bounds__(DN_THREADS) k_b_gram(const BDesc<FT>* __restrict__ d,
-                                                       const int* __restrict__ list,
+template <typename FT, int MAXT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_gram(const BDesc<FT>* __restrict__ d, BlkMap map,
                                                        const int* __restrict__ active, int j, int scaled)
 {
-    const int b = list[blockIdx.y];
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
     const int R = t.R;
     const bool last = j == t.nmode - 1;
-    gram_body<FT>(t.U[j], t.dims[j], R, t.G + (size_t)j * R * R, scaled ? t.lam : nullptr,
-                  scaled ? t.U[j] : nullptr, (scaled && last) ? t.M : nullptr, t.inner, blockIdx.x, gridDim.x);
+    gram_body<FT, MAXT>(t.U[j], t.dims[j], R, t.G + (size_t)j * R * R, scaled ? t.lam : nullptr,
+                        scaled ? t.U[j] : nullptr, (scaled && last) ? t.M : nullptr, t.inner, bx, nbx);
 }
 
 template <typename FT>
@@ -241,7 +262,20 @@ struct BatchImpl : BatchBase {
     cudaGraphExec_t gexec = nullptr;
     double g_eps = -1.0;
     int g_iters = -1;
-    int gx_apply = 1, gx_elem = 1;
+    // per mode: flattened block maps of the row kernels (apply, Gram) and of
+    // the element kernels (zero, copy)
+    // (mode, rank class): tensor list, row-block map, largest rank
+    int* d_clist[ALTOB_MAX_MODES][NRANK_CLASSES] = {};
+    int* d_rowpre[ALTOB_MAX_MODES][NRANK_CLASSES] = {};
+    int ncl[ALTOB_MAX_MODES][NRANK_CLASSES] = {};
+    int nrowblk[ALTOB_MAX_MODES][NRANK_CLASSES] = {};
+    int cmaxR[NRANK_CLASSES] = {};
+    int* d_elpre[ALTOB_MAX_MODES] = {nullptr};
+    int nelblk[ALTOB_MAX_MODES] = {0};
+    static constexpr u64 ROWS_PER_CTA = 512;
+    static constexpr u64 ELEMS_PER_CTA = 16384;
+    static constexpr u64 MAX_CTAS_PER_TENSOR = 64;
+    int launches_per_iter = 0;  // kernels one iteration launches (last count)
 
     ~BatchImpl() override
     {
@@ -251,7 +285,14 @@ struct BatchImpl : BatchBase {
         dfree(d_desc);
         dfree(d_active);
         dfree(d_iters);
-        for (int j = 0; j < ALTOB_MAX_MODES; ++j) dfree(d_list[j]);
+        for (int j = 0; j < ALTOB_MAX_MODES; ++j) {
+            dfree(d_list[j]);
+            dfree(d_elpre[j]);
+            for (int c = 0; c < NRANK_CLASSES; ++c) {
+                dfree(d_clist[j][c]);
+                dfree(d_rowpre[j][c]);
+            }
+        }
         dfree(d_scratch);
         for (auto& c : classes) c->free_args();
     }
@@ -355,28 +396,81 @@ struct BatchImpl : BatchBase {
     }
 
     size_t smem_solve() const { return (size_t)2 * maxR * maxR * sizeof(double); }
-    size_t smem_apply() const { return (size_t)(maxR * maxR + maxR) * sizeof(double); }
-    size_t smem_gram() const { return (size_t)(GR_ROWS * maxR + maxR) * sizeof(double); }
+    static size_t smem_apply(int R) { return (size_t)(R * R + R) * sizeof(double); }
+    static size_t smem_gram(int R) { return (size_t)(GR_ROWS * R + R) * sizeof(double); }
+
+    // row kernels of mode j, one launch per rank class
+    void launch_apply(int j, int nk, cudaStream_t st)
+    {
+        for (int c = 0; c < NRANK_CLASSES; ++c) {
+            if (!ncl[j][c]) continue;
+            const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
+            const size_t sm = smem_apply(cmaxR[c]);
+            const int g = nrowblk[j][c];
+            switch (c) {
+            case 0: k_b_apply<FT, 8, 1><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, nk); break;
+            case 1: k_b_apply<FT, 16, 1><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, nk); break;
+            case 2: k_b_apply<FT, 32, 1><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, nk); break;
+            case 3: k_b_apply<FT, 32, 2><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, nk); break;
+            default: k_b_apply<FT, 32, 4><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, nk); break;
+            }
+        }
+    }
+    void launch_gram(int j, int scaled, cudaStream_t st)
+    {
+        for (int c = 0; c < NRANK_CLASSES; ++c) {
+            if (!ncl[j][c]) continue;
+            const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
+            const size_t sm = smem_gram(cmaxR[c]);
+            const int g = nrowblk[j][c];
+            if (cmaxR[c] <= GR_SMALL) k_b_gram<FT, 1><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, scaled);
+            else k_b_gram<FT, 3><<<g, DN_THREADS, sm, st>>>(d_desc, m, d_active, j, scaled);
+        }
+    }
+    int row_launches(int j) const
+    {
+        int n = 0;
+        for (int c = 0; c < NRANK_CLASSES; ++c) n += ncl[j][c] ? 1 : 0;
+        return n;
+    }
+    altob_status set_smem_limits()
+    {
+        const int big = (int)smem_apply(SOLVE_MAX_RANK), bigg = (int)smem_gram(SOLVE_MAX_RANK);
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_solve<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * SOLVE_MAX_RANK * SOLVE_MAX_RANK * sizeof(double))));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_apply<FT, 32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_apply<FT, 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_gram<FT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigg));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_b_gram<FT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bigg));
+        return ALTOB_OK;
+    }
 
     // one CP-ALS iteration over all active tensors (cpd.hpp:96-160 per tensor)
     altob_status iteration(int nk, double eps, int max_iters, cudaStream_t st)
     {
+        int launches = 1;  // the fit
         for (int j = 0; j < maxN; ++j) {
             const int n = nlist[j];
             if (!n) continue;
             const int* L = d_list[j];
-            k_b_zero<FT><<<dim3(gx_elem, n), 256, 0, st>>>(d_desc, L, d_active, j);
-            for (auto& c : classes) ALTOB_TRY(mttkrp_class(*c, j, st));
-            k_b_copym<FT><<<dim3(gx_elem, n), 256, 0, st>>>(d_desc, L, d_active, j);
+            const BlkMap els = {L, d_elpre[j], n};
+            k_b_zero<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
+            for (auto& c : classes) {
+                ALTOB_TRY(mttkrp_class(*c, j, st));
+                launches += (c->d_args[j] && c->total_tiles[j]) ? 1 : 0;
+            }
+            launches += 5 + 2 * row_launches(j);
+            k_b_copym<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
             k_b_prep<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, j, nk);
             k_b_solve<FT><<<n, DN_THREADS, smem_solve(), st>>>(d_desc, L, d_active, j);
-            k_b_apply<FT><<<dim3(gx_apply, n), DN_THREADS, smem_apply(), st>>>(d_desc, L, d_active, j, nk);
+            launch_apply(j, nk, st);
             k_b_lambda<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, nk);
-            k_b_gram<FT><<<dim3(gx_apply, n), DN_THREADS, smem_gram(), st>>>(d_desc, L, d_active, j, 1);
+            launch_gram(j, 1, st);
             ALTOB_LAUNCH_CHECK();
         }
         k_b_fit<FT><<<count, DN_THREADS, 0, st>>>(d_desc, d_active, d_iters, eps, max_iters);
         ALTOB_LAUNCH_CHECK();
+        launches_per_iter = launches;
         return ALTOB_OK;
     }
 
@@ -416,9 +510,7 @@ struct BatchImpl : BatchBase {
     altob_status solve(int max_iters, double eps, double* fits, int* iters, int use_graph, cudaStream_t st) override
     {
         if (max_iters < 1 || max_iters > cap) return fail(ALTOB_ERR_ARG, "max_iters must be 1..fit capacity");
-        ALTOB_CUDA(cudaFuncSetAttribute(k_b_solve<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solve()));
-        ALTOB_CUDA(cudaFuncSetAttribute(k_b_apply<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_apply()));
-        ALTOB_CUDA(cudaFuncSetAttribute(k_b_gram<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_gram()));
+        ALTOB_TRY(set_smem_limits());
         // all tensors active, no fits yet; Grams of the initial factors
         std::vector<int> ones(count, 1);
         ALTOB_CUDA(cudaMemcpyAsync(d_active, ones.data(), count * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -426,7 +518,7 @@ struct BatchImpl : BatchBase {
         for (int j = 0; j < maxN; ++j) {
             if (!nlist[j]) continue;
             k_b_prep<FT><<<nlist[j], 128, 0, st>>>(d_desc, d_list[j], d_active, j, NORM_2);
-            k_b_gram<FT><<<dim3(gx_apply, nlist[j]), DN_THREADS, smem_gram(), st>>>(d_desc, d_list[j], d_active, j, 0);
+            launch_gram(j, 0, st);
         }
         ALTOB_LAUNCH_CHECK();
         // the first iteration normalises with the 2-norm, later ones with the max-norm
@@ -544,8 +636,8 @@ struct BatchImpl : BatchBase {
     void describe(std::string* out) const override
     {
         char line[320];
-        snprintf(line, sizeof(line), "tensors=%d classes=%zu max_modes=%d max_rank=%d\n", count, classes.size(),
-                 maxN, maxR);
+        snprintf(line, sizeof(line), "tensors=%d classes=%zu max_modes=%d max_rank=%d launches_per_iteration=%d\n",
+                 count, classes.size(), maxN, maxR, launches_per_iter);
         *out += line;
         for (auto& c : classes) {
             snprintf(line, sizeof(line), "class %s: tensors=%zu slots=%d lanes=%d chunks=%d tuned_ms=%.4f\n",
@@ -639,22 +731,48 @@ struct BatchImpl : BatchBase {
             dfree((void*)d_vals);
             dfree(d_nnz);
         }
-        // per-mode lists of the tensors that have that mode
-        u64 maxrows = 1;
+        // per-mode lists of the tensors that have that mode, element-block
+        // maps, and per rank class the row-block maps
+        for (int b = 0; b < n; ++b) {
+            const int c = rank_class(hdesc[b].R);
+            cmaxR[c] = std::max(cmaxR[c], hdesc[b].R);
+        }
         for (int j = 0; j < maxN; ++j) {
-            std::vector<int> L;
+            std::vector<int> L, ep(1, 0);
+            std::vector<int> CL[NRANK_CLASSES], RP[NRANK_CLASSES];
+            for (int c = 0; c < NRANK_CLASSES; ++c) RP[c].push_back(0);
             for (int b = 0; b < n; ++b)
                 if (ts[b]->nmode > j) {
                     L.push_back(b);
-                    maxrows = std::max<u64>(maxrows, ts[b]->dims[j]);
+                    const u64 I = ts[b]->dims[j], R = (u64)hdesc[b].R;
+                    const u64 rb = std::min<u64>(MAX_CTAS_PER_TENSOR, std::max<u64>(1, (I + ROWS_PER_CTA - 1) / ROWS_PER_CTA));
+                    const u64 eb = std::min<u64>(MAX_CTAS_PER_TENSOR,
+                                                 std::max<u64>(1, (I * R + ELEMS_PER_CTA - 1) / ELEMS_PER_CTA));
+                    ep.push_back(ep.back() + (int)eb);
+                    const int c = rank_class((int)R);
+                    CL[c].push_back(b);
+                    RP[c].push_back(RP[c].back() + (int)rb);
                 }
             nlist[j] = (int)L.size();
             if (L.empty()) continue;
+            nelblk[j] = ep.back();
             ALTOB_TRY(dmalloc_t(&d_list[j], L.size()));
+            ALTOB_TRY(dmalloc_t(&d_elpre[j], ep.size()));
             ALTOB_CUDA(cudaMemcpyAsync(d_list[j], L.data(), L.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(d_elpre[j], ep.data(), ep.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            for (int c = 0; c < NRANK_CLASSES; ++c) {
+                ncl[j][c] = (int)CL[c].size();
+                if (CL[c].empty()) continue;
+                nrowblk[j][c] = RP[c].back();
+                ALTOB_TRY(dmalloc_t(&d_clist[j][c], CL[c].size()));
+                ALTOB_TRY(dmalloc_t(&d_rowpre[j][c], RP[c].size()));
+                ALTOB_CUDA(cudaMemcpyAsync(d_clist[j][c], CL[c].data(), CL[c].size() * sizeof(int),
+                                           cudaMemcpyHostToDevice, st));
+                ALTOB_CUDA(cudaMemcpyAsync(d_rowpre[j][c], RP[c].data(), RP[c].size() * sizeof(int),
+                                           cudaMemcpyHostToDevice, st));
+            }
+            ALTOB_CUDA(cudaStreamSynchronize(st));
         }
-        gx_apply = (int)std::max<u64>(1, std::min<u64>(64, (maxrows + 255) / 256));
-        gx_elem = (int)std::max<u64>(1, std::min<u64>(64, (maxrows * maxR + 4095) / 4096));
         // shape classes: (order 3 | 4-5, lanes, elements per lane, chunks)
         std::map<std::string, ClassRun<FT>*> byk;
         for (int b = 0; b < n; ++b) {

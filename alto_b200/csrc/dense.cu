@@ -18,7 +18,17 @@ altob_status gram(const FT* U, u64 I, int R, double* G, const double* div, FT* U
     if (M) ALTOB_CUDA(cudaMemsetAsync(inner, 0, (size_t)R * sizeof(double), st));
     if (I == 0) return ALTOB_OK;
     size_t smem = (size_t)(GR_ROWS * R + R) * sizeof(double);
-    k_gram<FT><<<dn_grid(I, 4 * GR_ROWS), DN_THREADS, smem, st>>>(U, I, R, G, div, Uout, M, inner);
+    const int g = dn_grid(I, 4 * GR_ROWS);
+    static std::atomic<int> configured{0};
+    if (smem > 48 * 1024 && !configured.load()) {
+        ALTOB_CUDA(cudaFuncSetAttribute(k_gram<FT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)((GR_ROWS * 128 + 128) * sizeof(double))));
+        ALTOB_CUDA(cudaFuncSetAttribute(k_gram<FT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)((GR_ROWS * 128 + 128) * sizeof(double))));
+        configured.store(1);
+    }
+    if (R <= GR_SMALL) k_gram<FT, 1><<<g, DN_THREADS, smem, st>>>(U, I, R, G, div, Uout, M, inner);
+    else k_gram<FT, 3><<<g, DN_THREADS, smem, st>>>(U, I, R, G, div, Uout, M, inner);
     ALTOB_LAUNCH_CHECK();
     return ALTOB_OK;
 }
@@ -47,9 +57,25 @@ altob_status solve_setup(const double* G, int nmode, int target, int R, double* 
 }
 
 // ------------------------------------------------------------ row apply
-// U[i,:] <- U[i,:] W (FP64), four rows per warp step; column norms of the
+// U[i,:] <- U[i,:] W (FP64), lanes per row chosen by the rank; column norms of the
 // result are accumulated on the fly (2-norm: sum of squares; max-norm:
 // running max floored at 1, src/kruskal_model.cpp:264-305).
+
+template <typename FT, int LPR, int CJ>
+static altob_status launch_apply(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, int grid,
+                                 size_t smem, cudaStream_t st)
+{
+    static std::atomic<size_t> cfg{0};  // one per instantiation
+    if (smem > 48 * 1024 && smem > cfg.load()) {
+        ALTOB_CUDA(cudaFuncSetAttribute(k_apply<FT, LPR, CJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        size_t cur = cfg.load();
+        while (cur < smem && !cfg.compare_exchange_weak(cur, smem)) {
+        }
+    }
+    k_apply<FT, LPR, CJ><<<grid, DN_THREADS, smem, st>>>(U, I, R, W, (int)nk, colacc);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
 
 template <typename FT>
 altob_status apply_w(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, cudaStream_t st)
@@ -61,16 +87,14 @@ altob_status apply_w(FT* U, u64 I, int R, const double* W, NormKind nk, double* 
     }
     if (I == 0) return ALTOB_OK;
     size_t smem = (size_t)(R * R + R) * sizeof(double);
-    static std::atomic<size_t> cfg{0};  // one per FT instantiation
-    if (smem > 48 * 1024 && smem > cfg.load()) {
-        ALTOB_CUDA(cudaFuncSetAttribute(k_apply<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        size_t cur = cfg.load();
-        while (cur < smem && !cfg.compare_exchange_weak(cur, smem)) {
-        }
+    const int g = dn_grid(I, (DN_THREADS / 32) * AP_RW * 8);
+    switch (rank_class(R)) {
+    case 0: return launch_apply<FT, 8, 1>(U, I, R, W, nk, colacc, g, smem, st);
+    case 1: return launch_apply<FT, 16, 1>(U, I, R, W, nk, colacc, g, smem, st);
+    case 2: return launch_apply<FT, 32, 1>(U, I, R, W, nk, colacc, g, smem, st);
+    case 3: return launch_apply<FT, 32, 2>(U, I, R, W, nk, colacc, g, smem, st);
+    default: return launch_apply<FT, 32, 4>(U, I, R, W, nk, colacc, g, smem, st);
     }
-    k_apply<FT><<<dn_grid(I, (DN_THREADS / 32) * AP_RW * 8), DN_THREADS, smem, st>>>(U, I, R, W, (int)nk, colacc);
-    ALTOB_LAUNCH_CHECK();
-    return ALTOB_OK;
 }
 
 // ------------------------------------------------------------- small ops

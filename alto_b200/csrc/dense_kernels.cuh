@@ -31,26 +31,27 @@ static int dn_grid(u64 work, u64 per_block)
 
 constexpr int GR_TB = 4;
 constexpr int GR_ROWS = 64;
-constexpr int GR_MAXT = 3;  // tiles per thread (R <= 128)
+constexpr int GR_LD = 8;      // staged elements in flight per thread
+constexpr int GR_SMALL = 88;  // R <= 88: at most 253 tiles, one per thread
 
-template <typename FT>
+template <typename FT, int MAXT>
 __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R, double* __restrict__ G,
                                           const double* __restrict__ div, FT* __restrict__ Uout,
                                           const FT* __restrict__ M, double* __restrict__ inner, u64 bx, u64 nbx)
 {
     extern __shared__ double gsm[];
-    double* s = gsm;                     // GR_ROWS x R
-    double* si = gsm + GR_ROWS * R;      // R (inner partial)
+    double* s = gsm;                 // GR_ROWS x R
+    double* si = gsm + GR_ROWS * R;  // R (inner partial)
     const int tid = threadIdx.x;
     const int T = (R + GR_TB - 1) / GR_TB;
     const int NT = T * (T + 1) / 2;
     const int groups = NT >= DN_THREADS ? 1 : DN_THREADS / NT;
     const int grp = NT >= DN_THREADS ? 0 : tid / NT;
     const bool active = NT >= DN_THREADS || tid < groups * NT;
-    int ta[GR_MAXT], tb[GR_MAXT];
-    double acc[GR_MAXT][GR_TB * GR_TB];
+    int ta[MAXT], tb[MAXT];
+    double acc[MAXT][GR_TB * GR_TB];
 #pragma unroll
-    for (int k = 0; k < GR_MAXT; ++k) {
+    for (int k = 0; k < MAXT; ++k) {
         int t = NT >= DN_THREADS ? tid + k * DN_THREADS : tid % NT;
         if (NT < DN_THREADS && k > 0) t = NT;  // only one tile
         int a = 0;
@@ -60,32 +61,57 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
 #pragma unroll
         for (int e = 0; e < GR_TB * GR_TB; ++e) acc[k][e] = 0.0;
     }
-    if (M)
+    if (M) {
         for (int r = tid; r < R; r += DN_THREADS) si[r] = 0.0;
+        __syncthreads();
+    }
+    // element e of a chunk sits in column (e mod R); for R dividing the
+    // block size that column is the same for every element of a thread
+    const bool fixed_col = DN_THREADS % R == 0;
+    const int col_step = DN_THREADS % R;
+    double pin = 0.0;
     const u64 nchunks = (I + GR_ROWS - 1) / GR_ROWS;
     for (u64 ch = bx; ch < nchunks; ch += nbx) {
         const u64 r0 = ch * GR_ROWS;
-        const int nrows = (int)std::min<u64>(GR_ROWS, I - r0);
+        const int nrows = (int)min((u64)GR_ROWS, I - r0);
+        const int tot = GR_ROWS * R, valid = nrows * R;
+        const u64 base = r0 * (u64)R;  // a chunk is contiguous in memory
         __syncthreads();
-        for (int e = tid; e < GR_ROWS * R; e += DN_THREADS) {
-            const int row = e / R, col = e - row * R;
-            double x = 0.0;
-            if (row < nrows) {
-                const u64 gi = (r0 + row) * (u64)R + col;
-                x = (double)U[gi];
-                if (div) {
-                    x = x / div[col];
-                    if (Uout) Uout[gi] = (FT)x;
-                    x = (double)(FT)x;
-                }
-                if (M) atomicAdd(&si[col], x * (double)M[gi]);
+        int col = tid % R;
+        for (int e0 = 0; e0 < tot; e0 += GR_LD * DN_THREADS) {
+            FT v[GR_LD], mv[GR_LD];
+#pragma unroll
+            for (int q = 0; q < GR_LD; ++q) {
+                const int e = e0 + q * DN_THREADS + tid;
+                v[q] = e < valid ? U[base + e] : FT(0);
+                mv[q] = (M && e < valid) ? M[base + e] : FT(0);
             }
-            s[e] = x;
+#pragma unroll
+            for (int q = 0; q < GR_LD; ++q) {
+                const int e = e0 + q * DN_THREADS + tid;
+                if (e < tot) {
+                    double x = (double)v[q];
+                    if (e < valid) {
+                        if (div) {
+                            x = x / div[col];
+                            if (Uout) Uout[base + e] = (FT)x;
+                            x = (double)(FT)x;
+                        }
+                        if (M) {
+                            if (fixed_col) pin += x * (double)mv[q];
+                            else atomicAdd(&si[col], x * (double)mv[q]);
+                        }
+                    }
+                    s[e] = x;
+                }
+                col += col_step;
+                if (col >= R) col -= R;
+            }
         }
         __syncthreads();
         if (!active) continue;
 #pragma unroll
-        for (int k = 0; k < GR_MAXT; ++k) {
+        for (int k = 0; k < MAXT; ++k) {
             if (ta[k] < 0) continue;
             const int a0 = ta[k] * GR_TB, b0 = tb[k] * GR_TB;
             for (int row = grp; row < nrows; row += groups) {
@@ -105,7 +131,7 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
     }
     if (active) {
 #pragma unroll
-        for (int k = 0; k < GR_MAXT; ++k) {
+        for (int k = 0; k < MAXT; ++k) {
             if (ta[k] < 0) continue;
             const int a0 = ta[k] * GR_TB, b0 = tb[k] * GR_TB;
 #pragma unroll
@@ -121,17 +147,18 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
         }
     }
     if (M) {
+        if (fixed_col) atomicAdd(&si[tid % R], pin);
         __syncthreads();
         for (int r = tid; r < R; r += DN_THREADS) atomicAdd(&inner[r], si[r]);
     }
 }
 
-template <typename FT>
-static __global__ void __launch_bounds__(DN_THREADS) k_gram(const FT* __restrict__ U, u64 I, int R, double* __restrict__ G,
+template <typename FT, int MAXT>
+__global__ void __launch_bounds__(DN_THREADS) k_gram(const FT* __restrict__ U, u64 I, int R, double* __restrict__ G,
                                                      const double* __restrict__ div, FT* __restrict__ Uout,
                                                      const FT* __restrict__ M, double* __restrict__ inner)
 {
-    gram_body<FT>(U, I, R, G, div, Uout, M, inner, blockIdx.x, gridDim.x);
+    gram_body<FT, MAXT>(U, I, R, G, div, Uout, M, inner, blockIdx.x, gridDim.x);
 }
 
 
@@ -272,51 +299,57 @@ static __global__ void __launch_bounds__(DN_THREADS) k_solve_setup(const double*
     solve_body(G, nmode, target, R, W, info);
 }
 
+// Row apply: a row is held by LPR lanes, CJ columns per lane (column c =
+// l + LPR * j), AP_RW rows per lane group; 32 / LPR row groups per warp, so
+// small ranks keep every lane busy.  Row k of W is read from shared memory,
+// the u[i][k] operand is shuffled from the lane that holds it.
 constexpr int AP_RW = 4;
-constexpr int AP_CJ = 4;  // R <= 128
 
-template <typename FT>
+template <typename FT, int LPR, int CJ>
 __device__ __forceinline__ void apply_body(FT* __restrict__ U, u64 I, int R, const double* __restrict__ Wg, int nk,
                                            double* __restrict__ colacc, u64 bx, u64 nbx)
 {
+    constexpr int NG = 32 / LPR;  // row groups per warp
+    constexpr int ROWS_WARP = NG * AP_RW;
     extern __shared__ double asm_[];
-    double* W = asm_;          // R x R
+    double* W = asm_;           // R x R
     double* cr = asm_ + R * R;  // R column partials
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane / LPR, l = lane % LPR;
     for (int e = tid; e < R * R; e += DN_THREADS) W[e] = Wg[e];
     for (int r = tid; r < R; r += DN_THREADS) cr[r] = nk == NORM_MAX ? 1.0 : 0.0;
     __syncthreads();
-    const int CJ = (R + 31) / 32;
-    double part[AP_CJ];
+    double part[CJ];
 #pragma unroll
-    for (int j = 0; j < AP_CJ; ++j) part[j] = nk == NORM_MAX ? 1.0 : 0.0;
-    const u64 step = nbx * (DN_THREADS / 32) * AP_RW;
-    for (u64 i0 = (bx * (DN_THREADS / 32) + warp) * AP_RW; i0 < I; i0 += step) {
-        double u[AP_RW][AP_CJ], x[AP_RW][AP_CJ];
+    for (int j = 0; j < CJ; ++j) part[j] = nk == NORM_MAX ? 1.0 : 0.0;
+    const u64 step = nbx * (DN_THREADS / 32) * ROWS_WARP;
+    for (u64 w0 = (bx * (DN_THREADS / 32) + warp) * ROWS_WARP; w0 < I; w0 += step) {
+        const u64 i0 = w0 + (u64)g * AP_RW;
+        double u[AP_RW][CJ], x[AP_RW][CJ];
 #pragma unroll
         for (int rw = 0; rw < AP_RW; ++rw)
 #pragma unroll
-            for (int j = 0; j < AP_CJ; ++j) {
-                const int c = lane + 32 * j;
+            for (int j = 0; j < CJ; ++j) {
+                const int c = l + LPR * j;
                 const u64 i = i0 + rw;
-                u[rw][j] = (j < CJ && c < R && i < I) ? (double)U[i * R + c] : 0.0;
+                u[rw][j] = (c < R && i < I) ? (double)U[i * R + c] : 0.0;
                 x[rw][j] = 0.0;
             }
         for (int a = 0; a < R; ++a) {
-            const int ja = a >> 5, la = a & 31;
+            const int ja = a / LPR, la = g * LPR + (a % LPR);
             double ua[AP_RW];
 #pragma unroll
             for (int rw = 0; rw < AP_RW; ++rw) {
-                double v = 0.0;
+                double v = u[rw][0];
 #pragma unroll
-                for (int j = 0; j < AP_CJ; ++j)
+                for (int j = 1; j < CJ; ++j)
                     if (j == ja) v = u[rw][j];
                 ua[rw] = __shfl_sync(0xffffffffu, v, la);
             }
 #pragma unroll
-            for (int j = 0; j < AP_CJ; ++j) {
-                const int b = lane + 32 * j;
-                if (j < CJ && b < R) {
+            for (int j = 0; j < CJ; ++j) {
+                const int b = l + LPR * j;
+                if (b < R) {
                     const double w = W[a * R + b];
 #pragma unroll
                     for (int rw = 0; rw < AP_RW; ++rw) x[rw][j] += ua[rw] * w;
@@ -328,9 +361,9 @@ __device__ __forceinline__ void apply_body(FT* __restrict__ U, u64 I, int R, con
             const u64 i = i0 + rw;
             if (i >= I) continue;
 #pragma unroll
-            for (int j = 0; j < AP_CJ; ++j) {
-                const int b = lane + 32 * j;
-                if (j < CJ && b < R) {
+            for (int j = 0; j < CJ; ++j) {
+                const int b = l + LPR * j;
+                if (b < R) {
                     const FT y = (FT)x[rw][j];
                     U[i * R + b] = y;
                     const double yd = (double)y;
@@ -342,9 +375,9 @@ __device__ __forceinline__ void apply_body(FT* __restrict__ U, u64 I, int R, con
     }
     if (nk != NORM_NONE) {
 #pragma unroll
-        for (int j = 0; j < AP_CJ; ++j) {
-            const int b = lane + 32 * j;
-            if (j < CJ && b < R) {
+        for (int j = 0; j < CJ; ++j) {
+            const int b = l + LPR * j;
+            if (b < R) {
                 if (nk == NORM_2) atomicAdd(&cr[b], part[j]);
                 else atomic_max_pos(&cr[b], part[j]);
             }
@@ -357,12 +390,17 @@ __device__ __forceinline__ void apply_body(FT* __restrict__ U, u64 I, int R, con
     }
 }
 
-template <typename FT>
-static __global__ void __launch_bounds__(DN_THREADS) k_apply(FT* __restrict__ U, u64 I, int R, const double* __restrict__ Wg,
+template <typename FT, int LPR, int CJ>
+__global__ void __launch_bounds__(DN_THREADS) k_apply(FT* __restrict__ U, u64 I, int R, const double* __restrict__ Wg,
                                                       int nk, double* __restrict__ colacc)
 {
-    apply_body<FT>(U, I, R, Wg, nk, colacc, blockIdx.x, gridDim.x);
+    apply_body<FT, LPR, CJ>(U, I, R, Wg, nk, colacc, blockIdx.x, gridDim.x);
 }
+
+// Rank classes of the row kernels: (lanes per row, columns per lane) and
+// Gram tiles per thread.
+inline int rank_class(int R) { return R <= 8 ? 0 : R <= 16 ? 1 : R <= 32 ? 2 : R <= 64 ? 3 : 4; }
+constexpr int NRANK_CLASSES = 5;
 
 static __global__ void k_lambda(const double* acc, int R, int nk, double* lam)
 {

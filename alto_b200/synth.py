@@ -110,3 +110,34 @@ def random_factors(dims, rank, seed):
     """Uniform(0,1) factor matrices from numpy (for parity inputs)."""
     rng = np.random.default_rng(seed)
     return [rng.random((int(d), rank)) for d in dims]
+
+
+# ------------------------------------------------- batched / served streams
+
+def batch_shapes(count, seed, ranks=(8, 16, 32, 64), dim_range=(100, 50_000), nnz_range=(10_000, 2_000_000),
+                 orders=(3, 4, 5)):
+    """Shapes of the batched CP-ALS workload: order uniform over `orders`,
+    every dimension log-uniform in dim_range, nnz log-uniform in nnz_range,
+    rank uniform over `ranks`.  Returns [(dims, nnz, rank), ...]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nm = int(rng.choice(orders))
+        dims = tuple(int(round(np.exp(rng.uniform(np.log(dim_range[0]), np.log(dim_range[1]))))) for _ in range(nm))
+        nnz = int(round(np.exp(rng.uniform(np.log(nnz_range[0]), np.log(nnz_range[1])))))
+        out.append((dims, nnz, int(rng.choice(ranks))))
+    return out
+
+
+def uniform_coo_torch(dims, nnz, seed, device):
+    """`nnz` coordinates drawn uniformly (with replacement; repeated
+    coordinates stay separate nonzeros, which CP-ALS treats as their sum) and
+    values uniform in (0, 1], generated on `device`.  Returns (cidx int64
+    (nmode, nnz), vals float64)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    cidx = torch.stack([torch.randint(0, int(d), (nnz,), generator=g, device=device, dtype=torch.int64)
+                        for d in dims]).contiguous()
+    vals = 1.0 - torch.rand(nnz, generator=g, device=device, dtype=torch.float64)
+    return cidx, vals

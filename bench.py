@@ -18,6 +18,13 @@ reference's mttkrp_alto_par sweep (src/main.cpp:476-495) with fixed inputs.
   cpu_baseline = the reference's OpenMP mttkrp_alto_par on a bounded sample
 
 --impl reference times the reference's own CPU implementation instead.
+
+--workload batch runs the batched CP-ALS workload instead: 512 independent
+tensors (order 3, 4 or 5; dims log-uniform in [100, 50,000]; nnz log-uniform
+in [10,000, 2,000,000]; uniform coordinates; values uniform (0, 1]; rank from
+{8, 16, 32, 64}), 25 iterations each, solved by altob_batch_cpd_als in FP32
+(one step = the whole batch), beside the plain one-tensor-at-a-time FP64
+altob_cpd_als path on the same tensors and initial models.
 """
 import argparse
 import json
@@ -55,6 +62,10 @@ def parse():
     p.add_argument("--cpu-sample-draws", type=int, default=40_000_000)
     p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
     p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
+    p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch"])
+    p.add_argument("--batch-count", type=int, default=512)
+    p.add_argument("--batch-iters", type=int, default=25)
+    p.add_argument("--no-baseline", action="store_true", help="batch: skip the one-at-a-time FP64 arm")
     return p.parse_args()
 
 
@@ -407,9 +418,112 @@ def run_altob(args):
                            "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (no flush)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                             "kernel": "k_tiled (MTTKRP)", "launch_ms_per_mode": avg_ms,
+                             "kernel": "k_grouped (MTTKRP)", "launch_ms_per_mode": avg_ms,
                              "algorithmic_bytes_per_launch": bytes_per_mode},
                 "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args):
+    """Batched CP-ALS workload (see the module docstring)."""
+    import torch
+    import alto_b200 as ab
+    from alto_b200 import synth
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    iters = args.batch_iters
+    shapes = synth.batch_shapes(args.batch_count, SEED + 31 * rank)
+    t32, t64, init = [], [], []
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + rank)
+    for k, (dims, nnz, r) in enumerate(shapes):
+        cidx, vals = synth.uniform_coo_torch(dims, nnz, SEED * 1000 + k + 7919 * rank, dev)
+        d = np.array(dims, np.uint64)
+        t32.append(ab.create_alto_device(len(dims), d, nnz, cidx, vals.float(), nprtn=128, lit_bits=0,
+                                         val_dtype="f32", stream=stream))
+        if not args.no_baseline:
+            t64.append(ab.create_alto_device(len(dims), d, nnz, cidx, vals, nprtn=128, lit_bits=0,
+                                             val_dtype="f64", stream=stream))
+        init.append([torch.rand(int(x), r, dtype=torch.float64, device=dev, generator=g) for x in dims])
+        del cidx, vals
+    torch.cuda.synchronize()
+    nnz_total = sum(s[1] for s in shapes)
+    M32 = [ab.KruskalModel(list(s[0]), s[2], [u.float() for u in init[k]],
+                           torch.ones(s[2], dtype=torch.float32, device=dev)) for k, s in enumerate(shapes)]
+
+    def reset32():
+        for k, m in enumerate(M32):
+            for u, u0 in zip(m.U, init[k]):
+                u.copy_(u0)
+
+    b = ab.BatchCPD(t32, M32, fit_capacity=iters, stream=stream)
+    ta = time.perf_counter()
+    b.autotune(stream=stream)
+    tune_s = time.perf_counter() - ta
+    for _ in range(max(1, min(args.warmup, 3))):
+        reset32()
+        b.solve(iters, 0.0, stream=stream)
+    reset32()
+    torch.cuda.synchronize()
+    clk = ClockSampler()
+    clk.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 3))
+    ms_all = []
+    for _ in range(steps):
+        reset32()
+        e0.record(stream)
+        fits32, its32 = b.solve(iters, 0.0, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_all.append(e0.elapsed_time(e1))
+    clocks = clk.stop()
+    desc = b.describe()
+    launches_iter = int(desc.split("launches_per_iteration=")[1].split()[0])
+    ms = statistics.median(ms_all)
+    value = args.batch_count / (ms / 1e3)
+
+    base = None
+    fit_err = None
+    if not args.no_baseline:
+        M64 = [ab.KruskalModel(list(s[0]), s[2], [u.clone() for u in init[k]],
+                               torch.ones(s[2], dtype=torch.float64, device=dev)) for k, s in enumerate(shapes)]
+        ab.cpd_alto(t64[0], ab.KruskalModel(list(shapes[0][0]), shapes[0][2], [u.clone() for u in init[0]],
+                                            torch.ones(shapes[0][2], dtype=torch.float64, device=dev)), 2, 0.0)
+        torch.cuda.synchronize()
+        f64 = []
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for k in range(len(shapes)):
+            f64.append(ab.cpd_alto(t64[k], M64[k], iters, 0.0))
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bms = b0.elapsed_time(b1)
+        base = {"value": args.batch_count / (bms / 1e3), "unit": "solves/s", "ms": bms,
+                "path": "altob_cpd_als, FP64 model and values, one tensor after another on one stream"}
+        fit_err = {"final_max_abs": float(max(abs(fits32[k][iters - 1] - f64[k][-1]) for k in range(len(shapes)))),
+                   "all_iters_max_abs": float(max(np.max(np.abs(fits32[k][:iters] - f64[k])) for k in
+                                                  range(len(shapes)))),
+                   "tolerance": 1e-4}
+    b.close()
+    line = {"metric": "batched_cpals_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": ws,
+            "steps": steps, "warmup": max(1, min(args.warmup, 3)), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 Gram/solve/fit)", "data": "synthetic",
+            "config": {"workload": f"batched_cpals_{args.batch_count}x{iters}it", "tensors": args.batch_count,
+                       "iterations": iters, "nnz_total": nnz_total,
+                       "orders": dict((o, sum(1 for s in shapes if len(s[0]) == o)) for o in (3, 4, 5)),
+                       "ranks": dict((r, sum(1 for s in shapes if s[2] == r)) for r in (8, 16, 32, 64))},
+            "baseline_fp64_one_at_a_time": base,
+            "speedup_vs_fp64_one_at_a_time": (value / base["value"]) if base else None,
+            "fit_vs_fp64": fit_err, "autotune_s": tune_s, "schedule": desc,
+            "gpu_launches": steps * (1 + iters * launches_iter), "clocks": clocks,
+            "nnz_mode_rate_gnnz_s": sum(s[1] * len(s[0]) for s in shapes) * iters / (ms / 1e3) / 1e9}
+    if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
 
@@ -421,6 +535,8 @@ def main():
         return 0
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_altob(args)
 
 

@@ -52,8 +52,9 @@ def _solve_each(items, dtype, iters, eps):
     return out
 
 
-def _batch(items, dtype, iters, eps, autotune=False, use_graph=True):
-    models = [_model(dims, rank, 7 + k, dtype) for k, (dims, at, rank) in enumerate(items)]
+def _batch(items, dtype, iters, eps, autotune=False, use_graph=True, seeds=None):
+    seeds = seeds if seeds is not None else [7 + k for k in range(len(items))]
+    models = [_model(dims, rank, sd, dtype) for sd, (dims, at, rank) in zip(seeds, items)]
     b = ab.BatchCPD([at for _, at, _ in items], models, fit_capacity=iters)
     if autotune:
         b.autotune()
@@ -108,14 +109,22 @@ def test_batch_stopping_rule_per_tensor():
 
 
 def test_batch_result_same_alone_and_in_mix():
+    """FP32: fits alone and in the mix within 1e-4.  FP64: factors too (in
+    FP32 the atomics' order differs between the two launches, and random
+    rank-16..24 problems amplify that rounding in the factors, not the fit)."""
     items = _items(np.float32)
     iters = 6
-    mix_fits, _, mix_models = _batch(items, np.float32, iters, 1e-30)
+    mix_fits, _, _ = _batch(items, np.float32, iters, 1e-30)
     for k in (0, 3, 4):
-        alone_fits, _, alone_models = _batch([items[k]], np.float32, iters, 1e-30)
+        alone_fits, _, _ = _batch([items[k]], np.float32, iters, 1e-30, seeds=[7 + k])
         assert np.max(np.abs(alone_fits[0] - mix_fits[k])) < 1e-4
+    items = _items(np.float64)
+    mix_fits, _, mix_models = _batch(items, np.float64, iters, 1e-30)
+    for k in (0, 3, 4):
+        alone_fits, _, alone_models = _batch([items[k]], np.float64, iters, 1e-30, seeds=[7 + k])
+        assert np.max(np.abs(alone_fits[0] - mix_fits[k])) < 1e-9
         for n in range(len(alone_models[0].U)):
-            assert rel_fro(alone_models[0].U[n].cpu().numpy(), mix_models[k].U[n].cpu().numpy()) < 1e-3
+            assert rel_fro(alone_models[0].U[n].cpu().numpy(), mix_models[k].U[n].cpu().numpy()) < 1e-7
 
 
 def test_batch_autotune_keeps_factors_and_reports_classes():
