@@ -58,6 +58,26 @@ class _Coo(C.Structure):
 
 _lib = None
 
+
+class Request(C.Structure):
+    """altob_request (include/altob.h)."""
+    _fields_ = [("kind", C.c_int), ("nmode", C.c_int), ("dims", C.c_uint64 * MAX_MODES), ("nnz", C.c_uint64),
+                ("d_cidx", C.c_void_p), ("d_vals", C.c_void_p), ("vdtype", C.c_int), ("ftype", C.c_int),
+                ("rank", C.c_uint64), ("max_iters", C.c_int), ("max_inner", C.c_int), ("tol", C.c_double),
+                ("seed", C.c_uint), ("nprtn", C.c_int)]
+
+
+class Result(C.Structure):
+    """altob_result (include/altob.h)."""
+    _fields_ = [("status", C.c_int), ("iters", C.c_int), ("batch_size", C.c_int), ("fit", C.c_double),
+                ("loglik", C.c_double), ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double)]
+
+
+class ServerConfig(C.Structure):
+    """altob_server_config (include/altob.h)."""
+    _fields_ = [("hbm_budget", C.c_uint64), ("workers", C.c_int), ("max_batch", C.c_int), ("use_graph", C.c_int),
+                ("autotune", C.c_int), ("plain", C.c_int)]
+
 # name -> (restype, argtypes); the exported C ABI of include/altob.h
 _vp, _u64, _i, _d = C.c_void_p, C.c_uint64, C.c_int, C.c_double
 _u64p, _dp = C.POINTER(C.c_uint64), C.POINTER(C.c_double)
@@ -87,10 +107,17 @@ SIGNATURES = {
     "altob_cp_apr_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _i, _d, _d, _d, _d, _i, _dp, _vp]),
     "altob_kruskal_random_init": (_i, [_i, _u64p, _u64, C.c_uint, _i, _vp, _vp]),
     "altob_batch_create": (_i, [_vp, _i, _u64p, _i, _vp, _vp, _i, _vp, C.POINTER(_vp)]),
-    "altob_batch_autotune": (_i, [_vp, _vp]),
+    "altob_batch_autotune": (_i, [_vp, _i, _vp]),
     "altob_batch_cpd_als": (_i, [_vp, _i, _d, _dp, C.POINTER(_i), _i, _vp]),
     "altob_batch_describe": (_i, [_vp, C.c_char_p, C.c_size_t]),
     "altob_batch_destroy": (_i, [_vp]),
+    "altob_request_footprint": (_i, [C.POINTER(Request), _u64p]),
+    "altob_server_create": (_i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
+    "altob_server_clock": (C.c_double, [_vp]),
+    "altob_server_submit": (_i, [_vp, C.POINTER(Request), _u64p]),
+    "altob_server_wait": (_i, [_vp, C.c_uint64, C.POINTER(Result)]),
+    "altob_server_stats": (_i, [_vp, _u64p, _u64p, C.POINTER(_i), C.POINTER(_i)]),
+    "altob_server_destroy": (_i, [_vp]),
 }
 
 
@@ -471,8 +498,8 @@ class BatchCPD:
                                         C.byref(h)))
         self.handle = h.value
 
-    def autotune(self, stream=None):
-        _check(lib().altob_batch_autotune(self.handle, _stream_ptr(stream)))
+    def autotune(self, force=True, stream=None):
+        _check(lib().altob_batch_autotune(self.handle, int(bool(force)), _stream_ptr(stream)))
 
     def solve(self, max_iters, epsilon, use_graph=True, stream=None):
         """Returns (fits[count, max_iters], iters[count])."""

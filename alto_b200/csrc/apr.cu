@@ -8,6 +8,7 @@
 // below epsilon (skipped in bench mode), and KruskalModelNormalizeMode.  The
 // KKT violation and the log-likelihood accumulate in FP64.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -142,6 +143,20 @@ static altob_status loglik_impl(altob_tensor* t, FT** U, double* lam, double* co
     return ALTOB_OK;
 }
 
+// Precomputed Khatri-Rao rows (the reference's PRE build) when a mode runs
+// more than one inner iteration and the nnz x R buffer is small next to free
+// memory; ALTOB_APR_PHI=pre|otf forces either path.
+static bool apr_use_pre(const altob_tensor* t, int R, size_t fsz, int max_inner)
+{
+    const char* v = getenv("ALTOB_APR_PHI");
+    if (v && !strcmp(v, "otf")) return false;
+    if (v && !strcmp(v, "pre")) return true;
+    if (max_inner < 2) return false;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    return (double)t->nnz * R * fsz <= 0.25 * (double)fr;
+}
+
 template <typename FT>
 static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int max_iters, int max_inner,
                                 double eps, double eps_div_zero, double kappa_tol, double kappa, int dobench,
@@ -190,6 +205,12 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
     }
     std::vector<double> kkt_iter(max_iters + 1, 0.0), kmode(N, 0.0);
     std::vector<int> ninner(max_iters + 1, 0);
+    void* pi = nullptr;  // nnz x R precomputed rows
+    if (t->nnz && apr_use_pre(t, R, sizeof(FT), max_inner)) ALTOB_TRY(dmalloc(&pi, t->nnz * (size_t)R * sizeof(FT)));
+    struct PiFree {
+        void* p;
+        ~PiFree() { dfree(p); }
+    } pi_free{pi};
     int iter;
     for (iter = 0; iter < max_iters; ++iter) {
         bool converged = false;
@@ -203,9 +224,11 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
             }
             ALTOB_TRY(mul_cols<FT>(B, t->dims[n], R, s.lam, st));  // RedistributeLambda
             ALTOB_TRY(vec_fill(s.lam, R, 1.0, st));
+            if (pi) ALTOB_TRY(pi_device(t, n, ft, (void* const*)U, (u64)R, pi, st));
             for (int inner = 0; inner < max_inner; ++inner) {
                 ninner[iter]++;
-                ALTOB_TRY(phi_device(t, n, ft, (void* const*)U, (u64)R, eps_div_zero, Phi[n], st));
+                if (pi) ALTOB_TRY(phi_pre_device(t, n, ft, pi, B, (u64)R, eps_div_zero, Phi[n], st));
+                else ALTOB_TRY(phi_device(t, n, ft, (void* const*)U, (u64)R, eps_div_zero, Phi[n], st));
                 if (dobench) {
                     // no early exit: the violation of the last round is what the reference reports
                     ALTOB_CUDA(cudaMemsetAsync(s.kkt + n, 0, sizeof(double), st));

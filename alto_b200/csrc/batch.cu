@@ -19,6 +19,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "dense_kernels.cuh"
@@ -195,9 +196,33 @@ __global__ void k_b_sumsq(BDesc<FT>* __restrict__ d, const void* const* __restri
 
 // ---------------------------------------------------------------- host
 
+// Choices of the autotuner, remembered per (factor type, shape class) for
+// every later batch in the process.
+struct TuneChoice {
+    int hslots, lpn, ch;
+    float ms;
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneChoice> g_tune;
+
+static bool tune_lookup(const std::string& k, TuneChoice* out)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+static void tune_store(const std::string& k, const TuneChoice& c)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[k] = c;
+}
+
 template <typename FT>
 struct ClassRun {
-    int nm = 0;  // 3 or 0 (order 4-5)
+    int nm = 0;  // order 3-5 (static loops), or 0 (generic)
     altob_dtype vdt = ALTOB_F32;
     int lpn = 32, vec = 1, ch = 4;
     int hslots = 0;      // row slots of the grouped kernel (0: no grouping)
@@ -240,7 +265,7 @@ struct ClassRun {
 
 struct BatchBase {
     virtual ~BatchBase() {}
-    virtual altob_status autotune(cudaStream_t st) = 0;
+    virtual altob_status autotune(int force, cudaStream_t st) = 0;
     virtual altob_status solve(int max_iters, double eps, double* fits, int* iters, int use_graph,
                                cudaStream_t st) = 0;
     virtual void describe(std::string* out) const = 0;
@@ -368,7 +393,7 @@ struct BatchImpl : BatchBase {
         c.hslots = hslots;
         c.lpn = lpn;
         c.ch = ch;
-        c.smem = grouped_smem(hslots, c.nm == 3 ? 3 : ALTOB_MAX_MODES, sizeof(FT));
+        c.smem = grouped_smem(hslots, c.nm ? c.nm : ALTOB_MAX_MODES, sizeof(FT));
         ALTOB_TRY(build_class_args(c, st));
         BatchTiles<FT> bt;
         memset(&bt, 0, sizeof(bt));
@@ -560,7 +585,9 @@ struct BatchImpl : BatchBase {
     // layout) on the class's MTTKRP of every mode and keeps the fastest.  The
     // target factors are saved before and restored after, so the model the
     // caller passed in is unchanged.
-    altob_status autotune(cudaStream_t st) override
+    std::string tune_key(const ClassRun<FT>& c) const { return std::to_string(sizeof(FT)) + "|" + c.key; }
+
+    altob_status autotune(int force, cudaStream_t st) override
     {
         drop_graph();
         std::vector<int> ones(count, 1);
@@ -571,6 +598,8 @@ struct BatchImpl : BatchBase {
         altob_status s = ALTOB_OK;
         for (auto& cp : classes) {
             ClassRun<FT>& c = *cp;
+            TuneChoice known;
+            if (!force && tune_lookup(tune_key(c), &known)) continue;  // applied at creation
             // save the factors this class writes
             size_t bytes = 0;
             for (int b : c.members)
@@ -625,6 +654,7 @@ struct BatchImpl : BatchBase {
             s = set_choice(c, best.hs, best.lpn, best.ch, st);
             if (s != ALTOB_OK) break;
             c.tuned_ms = best_ms;
+            tune_store(tune_key(c), {best.hs, best.lpn, best.ch, best_ms});
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -781,9 +811,9 @@ struct BatchImpl : BatchBase {
             for (int m = 0; m < t->nmode; ++m) aligned = aligned && ptr_aligned16(hdesc[b].U[m]);
             TiledPlan pl;
             ALTOB_TRY(plan_tiled(t, (u64)hdesc[b].R, sizeof(FT), aligned, true, &pl));
-            const int nm = t->nmode == 3 ? 3 : 0;
+            const int nm = t->nmode >= 3 ? t->nmode : 0;
             char k[128];
-            snprintf(k, sizeof(k), "order=%s lanes=%d vec=%d chunks=%d", nm == 3 ? "3" : "4-5", pl.lpn, pl.vec,
+            snprintf(k, sizeof(k), "order=%d lanes=%d vec=%d chunks=%d", t->nmode, pl.lpn, pl.vec,
                      pl.ch);
             auto it = byk.find(k);
             if (it == byk.end()) {
@@ -800,7 +830,15 @@ struct BatchImpl : BatchBase {
             }
             it->second->members.push_back(b);
         }
-        for (auto& c : classes) ALTOB_TRY(set_choice(*c, c->hslots, c->lpn, c->ch, st));
+        for (auto& c : classes) {
+            TuneChoice known;
+            if (tune_lookup(tune_key(*c), &known)) {
+                c->tuned_ms = known.ms;
+                ALTOB_TRY(set_choice(*c, known.hslots, known.lpn, known.ch, st));
+            } else {
+                ALTOB_TRY(set_choice(*c, c->hslots, c->lpn, c->ch, st));
+            }
+        }
         ALTOB_CUDA(cudaStreamSynchronize(st));
         return ALTOB_OK;
     }
@@ -852,11 +890,11 @@ altob_status altob_batch_create(altob_tensor* const* tensors, int count, const u
     return ALTOB_OK;
 }
 
-altob_status altob_batch_autotune(altob_batch* b, void* stream)
+altob_status altob_batch_autotune(altob_batch* b, int force, void* stream)
 {
     if (!b) return fail(ALTOB_ERR_ARG, "NULL batch");
     StreamScope scope((cudaStream_t)stream);
-    return b->impl->autotune((cudaStream_t)stream);
+    return b->impl->autotune(force, (cudaStream_t)stream);
 }
 
 altob_status altob_batch_cpd_als(altob_batch* b, int max_iters, double epsilon, double* fits, int* iters,
@@ -880,8 +918,9 @@ altob_status altob_batch_describe(const altob_batch* b, char* buf, size_t len)
 
 altob_status altob_batch_destroy(altob_batch* b)
 {
+    // every call on a handle returns with its work finished, so the memory
+    // is released without waiting for the device
     if (!b) return ALTOB_OK;
-    ALTOB_CUDA(cudaDeviceSynchronize());
     delete b;
     return ALTOB_OK;
 }

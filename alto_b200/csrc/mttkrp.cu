@@ -66,7 +66,7 @@ altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, 
         pl->tile = GT_TILE;
         const int slots = env_int("ALTOB_GROUP_SLOTS", 2048);
         pl->hslots = cache ? std::max(32, std::min(floor_pow2(slots), 8192)) : 0;
-        const int mm = t->nmode == 3 ? 3 : ALTOB_MAX_MODES;
+        const int mm = t->nmode >= 3 ? t->nmode : ALTOB_MAX_MODES;
         pl->smem = grouped_smem(pl->hslots, mm, fsz);
         return ALTOB_OK;
     }
@@ -206,6 +206,158 @@ altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* 
     if (t->nnz == 0) return ALTOB_OK;
     return ft == ALTOB_F64 ? run_tiled<double>(t, mode, dU, dphi, R, true, eps, nullptr, true, st)
                            : run_tiled<float>(t, mode, dU, dphi, R, true, eps, nullptr, true, st);
+}
+
+// ------------------------------------------------- precomputed Phi rows
+// The Khatri-Rao row of every nonzero for target mode n (the product of the
+// other modes' factor rows), computed once and reused by every inner
+// iteration of that mode: the reference's PRE build of cp_apr_alto
+// (apr.hpp:1133-1171, precomp_row).  Same products in the same order as the
+// on-the-fly path, so both give the same Phi.
+
+template <typename FT>
+struct PiArgs {
+    KeySrc key;
+    Fields fld;
+    u64 nnz;
+    int nmode, target, R;
+    const FT* U[ALTOB_MAX_MODES];
+    FT* Pi;
+};
+
+template <typename FT, int NM, int VEC>
+__global__ void __launch_bounds__(256) k_pi(PiArgs<FT> a)
+{
+    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    const int nmode = NM ? NM : a.nmode;
+    const int cpr = a.R / VEC;  // VEC-wide chunks per row
+    const u64 total = a.nnz * (u64)cpr;
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
+        const u64 i = t / cpr;
+        const int c = (int)(t - i * cpr) * VEC;
+        const u64 lo = a.key.klo[i];
+        const u64 hi = a.key.khi ? a.key.khi[i] : (a.key.nrun ? key_hi(a.key, i) : 0);
+        FT x[VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) x[e] = FT(1);
+#pragma unroll
+        for (int m = 0; m < MM; ++m) {
+            if (NM == 0 && m >= nmode) break;
+            if (m == a.target) continue;
+            const u32 row = field(lo, hi, a.fld.pos[m], a.fld.mask[m]);
+            FT y[VEC];
+            vload<FT, VEC>(a.U[m] + (size_t)row * a.R + c, y);
+            vmul<FT, VEC>(x, y);
+        }
+        typedef typename VecT<FT, VEC>::T V;
+        *reinterpret_cast<V*>(a.Pi + i * a.R + c) = *reinterpret_cast<const V*>(x);
+    }
+}
+
+template <typename FT, int NM>
+static void launch_pi_nm(const PiArgs<FT>& a, int vec, int grid, cudaStream_t st)
+{
+    constexpr int V = 16 / sizeof(FT);
+    if (vec == V) k_pi<FT, NM, V><<<grid, 256, 0, st>>>(a);
+    else k_pi<FT, NM, 1><<<grid, 256, 0, st>>>(a);
+}
+
+template <typename FT>
+static altob_status pi_rows(altob_tensor* t, int mode, void* const* dU, u64 R, void* dpi, cudaStream_t st)
+{
+    PiArgs<FT> a;
+    memset(&a, 0, sizeof(a));
+    a.key = key_src(t);
+    a.fld = t->fld;
+    a.nnz = t->nnz;
+    a.nmode = t->nmode;
+    a.target = mode;
+    a.R = (int)R;
+    bool aligned = ptr_aligned16(dpi);
+    for (int m = 0; m < t->nmode; ++m) {
+        a.U[m] = (const FT*)dU[m];
+        aligned = aligned && ptr_aligned16(dU[m]);
+    }
+    a.Pi = (FT*)dpi;
+    constexpr int V = 16 / sizeof(FT);
+    const int vec = (aligned && R % V == 0) ? V : 1;
+    const u64 work = t->nnz * (R / vec);
+    const int grid = (int)std::max<u64>(1, std::min<u64>((work + 255) / 256, (u64)num_sms() * 16));
+    switch (t->nmode) {
+    case 3: launch_pi_nm<FT, 3>(a, vec, grid, st); break;
+    case 4: launch_pi_nm<FT, 4>(a, vec, grid, st); break;
+    case 5: launch_pi_nm<FT, 5>(a, vec, grid, st); break;
+    default: launch_pi_nm<FT, 0>(a, vec, grid, st); break;
+    }
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, void* dpi, cudaStream_t st)
+{
+    if (!t || !dU || !dpi) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    if (t->nnz == 0) return ALTOB_OK;
+    return ft == ALTOB_F64 ? pi_rows<double>(t, mode, dU, R, dpi, st) : pi_rows<float>(t, mode, dU, R, dpi, st);
+}
+
+// Phi of mode `mode` from precomputed rows `dpi` and the current factor B.
+template <typename FT, typename VT>
+static altob_status run_phi_pre_vt(altob_tensor* t, int mode, const void* dpi, const void* dB, void* dphi, u64 R,
+                                   double eps, cudaStream_t st)
+{
+    const bool aligned = ptr_aligned16(dpi) && ptr_aligned16(dB) && ptr_aligned16(dphi);
+    TiledPlan pl;
+    ALTOB_TRY(plan_tiled(t, R, sizeof(FT), aligned, true, &pl));
+    TiledArgs<FT> a;
+    memset(&a, 0, sizeof(a));
+    a.key = key_src(t);
+    a.vals = t->d_vals;
+    a.perm = nullptr;
+    a.nnz = t->nnz;
+    a.ntiles = (t->nnz + GT_TILE - 1) / GT_TILE;
+    a.nmode = t->nmode;
+    a.target = mode;
+    a.R = (int)R;
+    a.tile = GT_TILE;
+    a.hslots = pl.hslots ? pl.hslots : 2048;
+    a.eps = (FT)eps;
+    a.U[0] = (const FT*)dpi;
+    a.U[1] = (const FT*)dB;
+    a.out = (FT*)dphi;
+    a.fld = t->fld;
+    TiledCfg c;
+    c.lpn = pl.lpn;
+    c.vec = pl.vec;
+    c.ch = pl.ch;
+    c.phi = 1;
+    c.grouped = 1;
+    c.pre = 1;
+    c.smem = grouped_smem(a.hslots, 2, sizeof(FT));
+    c.grid = dim3(0);
+    int bps = 0;
+    ALTOB_TRY((launch_tiled<FT, VT>(a, c, st, &bps)));
+    if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "Phi kernel does not fit on an SM");
+    const u64 cap = (u64)bps * num_sms();
+    c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, cap)));
+    return launch_tiled<FT, VT>(a, c, st, nullptr);
+}
+
+altob_status phi_pre_device(altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const void* dB, u64 R,
+                            double eps, void* dphi, cudaStream_t st)
+{
+    if (!t || !dpi || !dB || !dphi) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_CUDA(cudaMemsetAsync(dphi, 0, t->dims[mode] * R * fsz, st));
+    if (t->nnz == 0) return ALTOB_OK;
+    const bool f64 = ft == ALTOB_F64;
+    if (t->vdt == ALTOB_U32)
+        return f64 ? run_phi_pre_vt<double, u32>(t, mode, dpi, dB, dphi, R, eps, st)
+                   : run_phi_pre_vt<float, u32>(t, mode, dpi, dB, dphi, R, eps, st);
+    if ((t->vdt == ALTOB_F64) != f64) return fail(ALTOB_ERR_UNSUPPORTED, "stored value dtype does not match the compute dtype");
+    return f64 ? run_phi_pre_vt<double, double>(t, mode, dpi, dB, dphi, R, eps, st)
+               : run_phi_pre_vt<float, float>(t, mode, dpi, dB, dphi, R, eps, st);
 }
 
 // Copies host factors into the handle's cached scratch (no per-call

@@ -420,6 +420,15 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 constexpr int GT_TILE = 1024;
 constexpr int GT_IPT = GT_TILE / MT_THREADS;
 
+// Record modes of a grouped kernel instance: NM = 3..5 (static order), 0
+// (any order, loops bounded at run time) or 1 (precomputed Khatri-Rao rows:
+// records hold the target row and the nonzero's position).
+template <int NM>
+constexpr int grouped_mm()
+{
+    return NM == 1 ? 2 : NM ? NM : ALTOB_MAX_MODES;
+}
+
 // 32-bit words of one shared record: output index, the other modes' indices,
 // the value, padding to 16 B.
 template <typename FT, int MM>
@@ -585,14 +594,15 @@ __device__ __forceinline__ void grouped_init(const GroupedSmem& g, int H)
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, const GroupedSmem& gs)
 {
-    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    constexpr bool PRE = NM == 1;  // a.U[0]: precomputed rows (nnz x R), a.U[1]: target factor
+    constexpr int MM = grouped_mm<NM>();
     constexpr int NPW = 32 / LPN;
     constexpr int RW = RecWords<FT, MM>::n;
     constexpr int NGRP = MT_WARPS * NPW;
     constexpr int IPG = GT_TILE / NGRP;  // sorted nonzeros per lane group
     constexpr int FW = (int)(sizeof(FT) / 4);
     const int R = a.R, H = a.hslots;
-    const int nmode = NM ? NM : a.nmode;
+    const int nmode = PRE ? 2 : NM ? NM : a.nmode;
     u32* rec = gs.rec;
     u32* srec = gs.srec;
     u32* tag = gs.tag;
@@ -610,9 +620,13 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
     const u32 lt_mask = (1u << lane) - 1u;
     const FT* Uo[MM - 1];
+    if constexpr (PRE) {
+        Uo[0] = a.U[0];
+    } else {
 #pragma unroll
-    for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : (k + 1 < MM ? k + 1 : k)];
-    const FT* Ut = a.U[target];
+        for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : (k + 1 < MM ? k + 1 : k)];
+    }
+    const FT* Ut = PRE ? a.U[1] : a.U[target];
     const int nother = nmode - 1;
     const u64 g0 = ti * (u64)GT_TILE;
     const int nvalid = (int)min((u64)GT_TILE, a.nnz - g0);
@@ -659,12 +673,18 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             else hi = g >= nstart ? hnext : hcur;
             u32* r = rec + (size_t)it * RW;
             u32 trow = 0;
+            if constexpr (PRE) {
+                trow = field(lo[k], hi, a.fld.pos[target], a.fld.mask[target]);
+                r[0] = trow;
+                r[1] = (u32)posv[k];
+            } else {
 #pragma unroll
-            for (int m = 0; m < MM; ++m) {
-                if (NM == 0 && m >= nmode) break;
-                const u32 c = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
-                r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
-                if (m == target) trow = c;
+                for (int m = 0; m < MM; ++m) {
+                    if (NM == 0 && m >= nmode) break;
+                    const u32 c = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
+                    r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
+                    if (m == target) trow = c;
+                }
             }
             const FT fv = (FT)vv[k];
             if constexpr (FW == 1) {
@@ -833,7 +853,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 __global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
 {
-    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 statics[2 + MT_WARPS];
     const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, a.hslots, statics);
@@ -859,7 +879,7 @@ struct BatchTiles {
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 __global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
 {
-    constexpr int MM = NM ? NM : ALTOB_MAX_MODES;
+    constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 statics[2 + MT_WARPS];
     const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, bt.hslots, statics);

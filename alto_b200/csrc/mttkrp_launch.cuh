@@ -10,10 +10,11 @@
 namespace altob {
 
 struct TiledCfg {
-    int lpn, vec, ch, phi;
-    int grouped;  // 1: k_grouped, 0: k_tiled
+    int lpn = 32, vec = 1, ch = 4, phi = 0;
+    int grouped = 1;  // 1: k_grouped, 0: k_tiled
+    int pre = 0;      // Phi from precomputed Khatri-Rao rows (grouped only)
     dim3 grid;
-    size_t smem;
+    size_t smem = 0;
 };
 
 template <typename FT, typename VT>
@@ -22,7 +23,7 @@ altob_status launch_tiled(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
 template <typename FT, typename VT>
 altob_status launch_atomic_cr(const CrArgsK<FT>& a, cudaStream_t st);
 
-// Batched grouped MTTKRP over the tensors of one shape class (nm = 3 or 0).
+// Batched grouped MTTKRP over the tensors of one shape class (nm = order 3-5, or 0).
 template <typename FT, typename VT>
 altob_status launch_batch(const BatchTiles<FT>& bt, int nm, const TiledCfg& c, cudaStream_t st, int* bps);
 
@@ -62,8 +63,15 @@ template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 altob_status launch_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     if (c.grouped) return launch_grouped<FT, VT, NM, LPN, VEC, CH, PHI>(a, c, st, bps);
-    static std::atomic<size_t> configured{0};
-    return launch_kernel(k_tiled<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
+    // k_tiled is built for order 3 and the generic order only
+    if constexpr (NM == 1) {
+        return fail(ALTOB_ERR_UNSUPPORTED, "precomputed rows need the grouped kernel");
+    } else if constexpr (NM == 4 || NM == 5) {
+        return launch_one<FT, VT, 0, LPN, VEC, CH, PHI>(a, c, st, bps);
+    } else {
+        static std::atomic<size_t> configured{0};
+        return launch_kernel(k_tiled<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
+    }
 }
 
 // (lanes per nonzero, elements per lane, chunks) -> kernel
@@ -128,16 +136,27 @@ altob_status launch_batch_shape(const BatchTiles<FT>& bt, const TiledCfg& c, cud
     altob_status launch_tiled<FT, VT>(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st,      \
                                       int* bps)                                                        \
     {                                                                                                  \
-        if (a.nmode == 3)                                                                              \
-            return c.phi ? launch_shape<FT, VT, 3, true>(a, c, st, bps)                                \
-                         : launch_shape<FT, VT, 3, false>(a, c, st, bps);                              \
+        if (c.pre) return launch_shape<FT, VT, 1, true>(a, c, st, bps);                                \
+        switch (a.nmode) {                                                                             \
+        case 3: return c.phi ? launch_shape<FT, VT, 3, true>(a, c, st, bps)                            \
+                             : launch_shape<FT, VT, 3, false>(a, c, st, bps);                          \
+        case 4: return c.phi ? launch_shape<FT, VT, 4, true>(a, c, st, bps)                            \
+                             : launch_shape<FT, VT, 4, false>(a, c, st, bps);                          \
+        case 5: return c.phi ? launch_shape<FT, VT, 5, true>(a, c, st, bps)                            \
+                             : launch_shape<FT, VT, 5, false>(a, c, st, bps);                          \
+        }                                                                                              \
         return c.phi ? launch_shape<FT, VT, 0, true>(a, c, st, bps) : launch_shape<FT, VT, 0, false>(a, c, st, bps); \
     }                                                                                                  \
     template <>                                                                                        \
     altob_status launch_batch<FT, VT>(const BatchTiles<FT>& bt, int nm, const TiledCfg& c, cudaStream_t st, \
                                       int* bps)                                                        \
     {                                                                                                  \
-        return nm == 3 ? launch_batch_shape<FT, VT, 3>(bt, c, st, bps) : launch_batch_shape<FT, VT, 0>(bt, c, st, bps); \
+        switch (nm) {                                                                                  \
+        case 3: return launch_batch_shape<FT, VT, 3>(bt, c, st, bps);                                  \
+        case 4: return launch_batch_shape<FT, VT, 4>(bt, c, st, bps);                                  \
+        case 5: return launch_batch_shape<FT, VT, 5>(bt, c, st, bps);                                  \
+        }                                                                                              \
+        return launch_batch_shape<FT, VT, 0>(bt, c, st, bps);                                          \
     }                                                                                                  \
     template <>                                                                                        \
     altob_status launch_atomic_cr<FT, VT>(const CrArgsK<FT>& a, cudaStream_t st)                       \

@@ -17,5 +17,11 @@ altob_status mttkrp_device(altob_tensor* t, int mode, altob_dtype ft, void* cons
                            altob_algo algo, cudaStream_t st);
 altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, double eps,
                         void* dphi, cudaStream_t st);
+// Khatri-Rao rows of every nonzero for `mode` (nnz x R, ALTO order) and Phi
+// computed from them (CP-APR with precomputed rows).
+altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, void* dpi,
+                       cudaStream_t st);
+altob_status phi_pre_device(altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const void* dB, u64 R,
+                            double eps, void* dphi, cudaStream_t st);
 
 }  // namespace altob

@@ -141,3 +141,59 @@ def uniform_coo_torch(dims, nnz, seed, device):
                         for d in dims]).contiguous()
     vals = 1.0 - torch.rand(nnz, generator=g, device=device, dtype=torch.float64)
     return cidx, vals
+
+
+def poisson_kruskal_torch(dims, rank, total_counts, seed, device, shape=0.3, scale=1.0):
+    """poisson_kruskal on `device`: each of `total_counts` events picks a
+    component uniformly, then one index per mode from that component's
+    Gamma(shape, scale) column (normalised); repeated coordinates are merged
+    into INT32 counts.  Returns (cidx int64 (nmode, nnz), vals int32)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    rng = np.random.default_rng(seed)  # the factor columns (dims x rank) are small: drawn on the host
+    comp = torch.randint(0, rank, (total_counts,), generator=g, device=device)
+    idx = []
+    for d in dims:
+        d = int(d)
+        A = torch.from_numpy(rng.gamma(shape, scale, size=(d, rank))).to(device)
+        A /= A.sum(dim=0, keepdim=True)
+        cdf = torch.cumsum(A, 0)
+        cdf /= cdf[-1:].clone()
+        # column r of the flattened table holds r + cdf[:, r], so one sorted search serves every component
+        flat = (cdf.t() + torch.arange(rank, device=device, dtype=torch.float64)[:, None]).reshape(-1)
+        u = torch.rand(total_counts, generator=g, device=device, dtype=torch.float64) * (1 - 1e-12)
+        pos = torch.searchsorted(flat, u + comp.double(), right=True)
+        idx.append((pos - comp * d).clamp_(0, d - 1))
+    # merge repeated coordinates: lexicographic order by stable sorts, last mode first
+    order = torch.arange(total_counts, device=device)
+    for i in reversed(idx):
+        order = order[torch.sort(i[order], stable=True).indices]
+    cs = torch.stack([i[order] for i in idx])
+    new = torch.ones(total_counts, dtype=torch.bool, device=device)
+    new[1:] = (cs[:, 1:] != cs[:, :-1]).any(dim=0)
+    seg = torch.cumsum(new.to(torch.int64), 0) - 1
+    nnz = int(seg[-1].item()) + 1
+    counts = torch.zeros(nnz, dtype=torch.int32, device=device).index_add_(0, seg, torch.ones_like(seg, dtype=torch.int32))
+    return cs[:, new].contiguous(), counts
+
+
+def served_stream(count, seed, rate=200.0, als_frac=0.7, ranks=(16, 32, 64), nnz_range=(50_000, 20_000_000),
+                  dim_range=(100, 50_000), orders=(3, 4, 5), apr_rank=8):
+    """The served request stream: Poisson arrivals at `rate` per second;
+    each request CP-ALS (probability als_frac; uniform coordinates, values
+    uniform (0, 1]) or CP-APR (Poisson counts from a rank-`apr_rank`
+    Gamma(0.3, 1) Kruskal model); order uniform over `orders`, dimensions
+    log-uniform in dim_range, nnz log-uniform in nnz_range, rank uniform
+    over `ranks`.  Returns [(arrival_s, kind, dims, nnz, rank, seed), ...]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += rng.exponential(1.0 / rate)
+        kind = "als" if rng.random() < als_frac else "apr"
+        nm = int(rng.choice(orders))
+        dims = tuple(int(round(np.exp(rng.uniform(np.log(dim_range[0]), np.log(dim_range[1]))))) for _ in range(nm))
+        nnz = int(round(np.exp(rng.uniform(np.log(nnz_range[0]), np.log(nnz_range[1])))))
+        out.append((t, kind, dims, nnz, int(rng.choice(ranks)), int(rng.integers(1, 2**31))))
+    return out

@@ -25,6 +25,13 @@ in [10,000, 2,000,000]; uniform coordinates; values uniform (0, 1]; rank from
 {8, 16, 32, 64}), 25 iterations each, solved by altob_batch_cpd_als in FP32
 (one step = the whole batch), beside the plain one-tensor-at-a-time FP64
 altob_cpd_als path on the same tensors and initial models.
+
+--workload serve replays a served request stream: Poisson arrivals at 200/s,
+70% CP-ALS (tensors as in the batch workload, nnz log-uniform in [50,000,
+20,000,000]) and 30% CP-APR (INT32 Poisson counts from a rank-8 Gamma(0.3, 1)
+Kruskal model), rank from {16, 32, 64}, tolerance 1e-4, at most 50
+iterations, 150 GB HBM budget; FP32 served path (concurrent workers, CP-ALS
+batching) beside the plain one-at-a-time FP64 path on the same stream.
 """
 import argparse
 import json
@@ -62,7 +69,10 @@ def parse():
     p.add_argument("--cpu-sample-draws", type=int, default=40_000_000)
     p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
     p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
-    p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch"])
+    p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch", "serve"])
+    p.add_argument("--serve-requests", type=int, default=60)
+    p.add_argument("--serve-workers", type=int, default=4)
+    p.add_argument("--serve-batch", type=int, default=32)
     p.add_argument("--batch-count", type=int, default=512)
     p.add_argument("--batch-iters", type=int, default=25)
     p.add_argument("--no-baseline", action="store_true", help="batch: skip the one-at-a-time FP64 arm")
@@ -528,6 +538,87 @@ def run_batch(args):
     return 0
 
 
+def run_serve(args):
+    """Served decomposition stream (see the module docstring)."""
+    import torch
+    import alto_b200 as ab
+    from alto_b200 import serve, synth
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = synth.served_stream(args.serve_requests, SEED + 17 * rank)
+    inputs = []
+    for k, (at, kind, dims, nnz, r, seed) in enumerate(stream):
+        if kind == "als":
+            cidx, vals = synth.uniform_coo_torch(dims, nnz, seed, dev)
+            inputs.append((kind, dims, cidx, vals.float(), vals, r, seed))
+        else:
+            cidx, cnt = synth.poisson_kruskal_torch(dims, 8, nnz, seed, dev)
+            inputs.append((kind, dims, cidx, cnt, cnt, r, seed))
+    torch.cuda.synchronize()
+    arrivals = [x[0] for x in stream]
+
+    def requests(ftype):
+        out = []
+        for kind, dims, cidx, v32, v64, r, seed in inputs:
+            vals = v32 if ftype == ab.F32 else v64
+            k = serve.ALS if kind == "als" else serve.APR
+            req = serve.Server.make_request(k, dims, cidx, vals, r, 50, 1e-4, seed, ftype, max_inner=10)
+            out.append((req, (cidx, vals)))
+        return out
+
+    # served path; a short warm-up stream first tunes the shape classes
+    srv = serve.Server(hbm_budget_gb=150, workers=args.serve_workers, max_batch=args.serve_batch)
+    reqs = requests(ab.F32)
+    nw = min(len(reqs), 12)
+    serve.replay(srv, reqs[:nw], [0.0] * nw)
+    clk = ClockSampler()
+    clk.start()
+    time.sleep(0.3)
+    res, summ = serve.replay(srv, reqs, arrivals)
+    clocks = clk.stop()
+    for kind in ("als", "apr"):
+        lat = [r["latency"] for (k, *_), r in zip(inputs, res) if k == kind]
+        summ[f"{kind}_p50_ms"] = float(np.percentile(lat, 50) * 1e3) if lat else None
+        summ[f"{kind}_iters_mean"] = float(np.mean([r["iters"] for (k, *_), r in zip(inputs, res) if k == kind])) \
+            if lat else None
+    peak = srv.stats()["peak_bytes"]
+    srv.close()
+    base = None
+    agree = None
+    if not args.no_baseline:
+        srv = serve.Server(hbm_budget_gb=150, workers=1, max_batch=1, plain=True)
+        bres, bsumm = serve.replay(srv, requests(ab.F64), arrivals)
+        srv.close()
+        base = dict(bsumm, path="plain one-at-a-time FP64: altob_cpd_als / altob_cp_apr, one worker, no batching")
+        for kind in ("als", "apr"):
+            base[f"{kind}_service_s"] = float(sum(b["t_end"] - b["t_start"] for (k, *_), b in zip(inputs, bres)
+                                                  if k == kind))
+        als_d = [abs(a["fit"] - b["fit"]) for (kind, *_), a, b in zip(inputs, res, bres) if kind == "als"]
+        apr_d = [abs(a["loglik"] - b["loglik"]) / max(1e-300, abs(b["loglik"]))
+                 for (kind, *_), a, b in zip(inputs, res, bres) if kind == "apr"]
+        agree = {"als_fit_within_1e-4": int(sum(d < 1e-4 for d in als_d)), "als": len(als_d),
+                 "als_fit_max_abs": float(max(als_d)) if als_d else None,
+                 "als_fit_median_abs": float(np.median(als_d)) if als_d else None,
+                 "apr_loglik_within_1e-4_rel": int(sum(d < 1e-4 for d in apr_d)), "apr": len(apr_d),
+                 "apr_loglik_max_rel": float(max(apr_d)) if apr_d else None}
+    line = {"metric": "served_solves_per_s", "value": summ["solves_per_s"], "unit": "solves/s", "n_gpus": ws,
+            "steps": 1, "warmup": 1, "ms_per_step": summ["makespan_s"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 Gram/solve/fit/KKT/LL)",
+            "data": "synthetic",
+            "config": {"workload": f"served_stream_{len(inputs)}req_200rps", "requests": len(inputs),
+                       "als": sum(1 for x in inputs if x[0] == "als"), "apr": sum(1 for x in inputs if x[0] == "apr"),
+                       "nnz_total": int(sum(int(x[3].shape[0]) for x in inputs)), "hbm_budget_gb": 150,
+                       "workers": args.serve_workers, "max_batch": args.serve_batch},
+            "served": summ, "peak_admitted_bytes": peak, "baseline_fp64_one_at_a_time": base,
+            "speedup_vs_fp64_one_at_a_time": (summ["solves_per_s"] / base["solves_per_s"]) if base else None,
+            "agreement_vs_fp64": agree, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.cpu_baseline_file:
@@ -537,6 +628,8 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_altob(args)
 
 

@@ -246,10 +246,12 @@ ALTOB_API altob_status altob_batch_create(altob_tensor* const* tensors, int coun
                                           void* const* const* d_factors,
                                           void* const* d_lambda, int fit_capacity,
                                           void* stream, altob_batch** out);
-/* Picks, per shape class (order 3 or 4-5, lanes per nonzero, elements per
+/* Picks, per shape class (order, lanes per nonzero, elements per
  * lane), the row-slot count and lane layout of the batched MTTKRP by timing
- * every candidate on that class; leaves the factors unchanged. */
-ALTOB_API altob_status altob_batch_autotune(altob_batch* b, void* stream);
+ * every candidate on that class; leaves the factors unchanged.  Choices are
+ * remembered per class for the rest of the process and applied to later
+ * batches at creation; force = 0 tunes only classes without one. */
+ALTOB_API altob_status altob_batch_autotune(altob_batch* b, int force, void* stream);
 /* fits: count x max_iters (row b = tensor b, 0 after its last iteration) or
  * NULL; iters: count or NULL.  use_graph = 0 launches every iteration
  * directly (same results).  Synchronous on `stream`. */
@@ -259,6 +261,69 @@ ALTOB_API altob_status altob_batch_cpd_als(altob_batch* b, int max_iters, double
 /* Text description of the shape classes and their chosen schedules. */
 ALTOB_API altob_status altob_batch_describe(const altob_batch* b, char* buf, size_t len);
 ALTOB_API altob_status altob_batch_destroy(altob_batch* b);
+
+/* ---- decomposition server ----------------------------------------------
+ * No counterpart in the reference.  A request loop over the solvers above:
+ * requests are queued in arrival order and admitted against an HBM budget
+ * (footprint estimated by altob_request_footprint); `workers` requests or
+ * batches run at once, each worker on its own CUDA stream.  A worker that
+ * admits a CP-ALS request takes the queued CP-ALS requests behind it with
+ * the same dtypes, iteration limit and tolerance (up to max_batch, within
+ * the budget) into one altob_batch solve.  With plain = 1 every request runs
+ * alone through altob_cpd_als / altob_cp_apr (no batching).  Factors are
+ * initialised on the device from the request's seed, identically alone or in
+ * a batch.  The request's COO arrays (device, as for altob_create_device)
+ * must stay valid until altob_server_wait returns for it. */
+typedef enum { ALTOB_REQ_CPD_ALS = 0, ALTOB_REQ_CP_APR = 1 } altob_req_kind;
+
+typedef struct {
+    altob_req_kind kind;
+    int nmode;
+    uint64_t dims[ALTOB_MAX_MODES];
+    uint64_t nnz;
+    const void* d_cidx;  /* device, nmode x nnz uint64 (mode-major) */
+    const void* d_vals;  /* device, nnz values of vdtype */
+    altob_dtype vdtype;  /* F32 / F64 values (CP-ALS), U32 counts (CP-APR) */
+    altob_dtype ftype;   /* model dtype, F32 or F64 */
+    uint64_t rank;       /* 1..112 */
+    int max_iters;       /* CP-ALS iterations / CP-APR outer iterations */
+    int max_inner;       /* CP-APR inner iterations */
+    double tol;          /* CP-ALS |fit change| / CP-APR KKT tolerance */
+    unsigned seed;       /* factor initialisation */
+    int nprtn;           /* ALTO partitions (0: 128) */
+} altob_request;
+
+typedef struct {
+    altob_status status;
+    int iters;        /* CP-ALS iterations / CP-APR outer iterations run */
+    int batch_size;   /* requests solved together with this one */
+    double fit;       /* final fit (CP-APR: its least-squares fit) */
+    double loglik;    /* CP-APR log-likelihood */
+    double t_submit;  /* server clock, seconds */
+    double t_start;
+    double t_end;
+} altob_result;
+
+typedef struct {
+    uint64_t hbm_budget; /* bytes admitted requests may use together */
+    int workers;         /* requests or batches in flight (1..64) */
+    int max_batch;       /* CP-ALS requests per batched solve */
+    int use_graph;       /* replay batched iterations from a CUDA graph */
+    int autotune;        /* tune unseen shape classes on first use */
+    int plain;           /* 1: no batching, altob_cpd_als per request */
+} altob_server_config;
+
+typedef struct altob_server altob_server;
+ALTOB_API altob_status altob_request_footprint(const altob_request* r, uint64_t* bytes);
+ALTOB_API altob_status altob_server_create(const altob_server_config* cfg, altob_server** out);
+ALTOB_API double altob_server_clock(const altob_server* s);
+ALTOB_API altob_status altob_server_submit(altob_server* s, const altob_request* r, uint64_t* id);
+/* Blocks until request `id` completes; each id can be waited for once. */
+ALTOB_API altob_status altob_server_wait(altob_server* s, uint64_t id, altob_result* out);
+ALTOB_API altob_status altob_server_stats(const altob_server* s, uint64_t* used_bytes,
+                                          uint64_t* peak_bytes, int* queued, int* running);
+/* Finishes the queued requests, then stops the workers. */
+ALTOB_API altob_status altob_server_destroy(altob_server* s);
 
 /* ---- tensor files ------------------------------------------------------
  * Replaces ImportSparseTensor (sptensor.cpp:165-258).  The .tns reader

@@ -138,7 +138,7 @@ def test_batch_autotune_keeps_factors_and_reports_classes():
         for u, v in zip(m.U, bu):
             assert torch.equal(u, v)
     text = b.describe()
-    assert "order=3" in text and "order=4-5" in text and "tuned_ms" in text
+    assert all(f"order={o}" in text for o in (3, 4, 5)) and "tuned_ms" in text
     b.close()
 
 

@@ -71,8 +71,12 @@ def test_gpu_cpd_device_model_matches_oracle(oracle):
         assert rel_fro(dU[n].cpu().numpy(), U[n]) < 1e-8
 
 
+@pytest.mark.parametrize("phi", ["pre", "otf"])
 @pytest.mark.parametrize("name", ["apr_bench", "apr_eps"])
-def test_gpu_cp_apr_fp64_matches_reference_fixture(name):
+def test_gpu_cp_apr_fp64_matches_reference_fixture(name, phi, monkeypatch):
+    """Both Phi paths (precomputed Khatri-Rao rows, on the fly) against the
+    reference's own output."""
+    monkeypatch.setenv("ALTOB_APR_PHI", phi)
     g = load_golden(name)
     rank = int(g["rank"])
     at = ab.create_alto(_coo(g["dims"], g["cidx"], g["vals"]), int(g["nprtn"]), 64, val_dtype="u32")
@@ -87,7 +91,9 @@ def test_gpu_cp_apr_fp64_matches_reference_fixture(name):
         assert rel_fro(M.U[n], g[f"U{n}"]) < 1e-8
 
 
-def test_gpu_cp_apr_early_exit_and_fp32(oracle):
+@pytest.mark.parametrize("phi", ["pre", "otf"])
+def test_gpu_cp_apr_early_exit_and_fp32(oracle, phi, monkeypatch):
+    monkeypatch.setenv("ALTOB_APR_PHI", phi)
     dims, cidx, vals = synth.poisson_kruskal((200, 150, 100, 20), 6, 200_000, seed=6)
     rank = 8
     U, lam = oracle.random_init(dims, rank, 4)
