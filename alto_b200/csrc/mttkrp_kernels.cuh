@@ -419,6 +419,18 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 
 constexpr int GT_TILE = 1024;
 constexpr int GT_IPT = GT_TILE / MT_THREADS;
+// Nonzeros a lane group takes per step in the run phase of the grouped kernels.
+#ifndef GT_NZS
+#define GT_NZS 2
+#endif
+
+// Launch bounds of the grouped kernels; a build may ask for a minimum number
+// of resident blocks per SM (caps registers) with -DGT_MIN_BLOCKS=n.
+#ifdef GT_MIN_BLOCKS
+#define GT_BOUNDS __launch_bounds__(MT_THREADS, GT_MIN_BLOCKS)
+#else
+#define GT_BOUNDS __launch_bounds__(MT_THREADS)
+#endif
 
 // Record modes of a grouped kernel instance: NM = 3..5 (static order), 0
 // (any order, loops bounded at run time) or 1 (precomputed Khatri-Rao rows:
@@ -794,36 +806,30 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     const int p0 = grp * IPG;
     const int pend = min(p0 + IPG, nvalid);
     int p = p0;
-    // two nonzeros per step: both gathers in flight before the run logic
-    for (; p + 1 < pend; p += 2) {
-        u32 w0[RW], w1[RW];
-        load_rec<FT, RW>(srec + (size_t)p * RW, w0);
-        load_rec<FT, RW>(srec + (size_t)(p + 1) * RW, w1);
-        FT x0[CH][VEC], x1[CH][VEC];
-        nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
-        nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w1, Uo, Ut, R, sub, nother, a.eps, gmask, x1);
-        if (w0[0] != prow) {
-            if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-            prow = w0[0];
+    // GT_NZS nonzeros per step: all their gathers in flight before the run logic
+    for (; p + GT_NZS - 1 < pend; p += GT_NZS) {
+        u32 w[GT_NZS][RW];
 #pragma unroll
-            for (int ch = 0; ch < CH; ++ch)
+        for (int q = 0; q < GT_NZS; ++q) load_rec<FT, RW>(srec + (size_t)(p + q) * RW, w[q]);
+        FT x[GT_NZS][CH][VEC];
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
-        } else {
-            run_add<FT, VEC, CH>(racc, x0);
-        }
-        if (w1[0] != prow) {
-            flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
-            prow = w1[0];
+        for (int q = 0; q < GT_NZS; ++q)
+            nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w[q], Uo, Ut, R, sub, nother, a.eps, gmask, x[q]);
 #pragma unroll
-            for (int ch = 0; ch < CH; ++ch)
+        for (int q = 0; q < GT_NZS; ++q) {
+            if (w[q][0] != prow) {
+                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+                prow = w[q][0];
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) racc[ch][e] = x1[ch][e];
-        } else {
-            run_add<FT, VEC, CH>(racc, x1);
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) racc[ch][e] = x[q][ch][e];
+            } else {
+                run_add<FT, VEC, CH>(racc, x[q]);
+            }
         }
     }
-    if (p < pend) {
+    for (; p < pend; ++p) {
         u32 w0[RW];
         load_rec<FT, RW>(srec + (size_t)p * RW, w0);
         FT x0[CH][VEC];
@@ -851,7 +857,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
 }
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
+__global__ void GT_BOUNDS k_grouped(TiledArgs<FT> a)
 {
     constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -877,7 +883,7 @@ struct BatchTiles {
 };
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
+__global__ void GT_BOUNDS k_grouped_batch(BatchTiles<FT> bt)
 {
     constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];

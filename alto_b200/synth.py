@@ -178,22 +178,25 @@ def poisson_kruskal_torch(dims, rank, total_counts, seed, device, shape=0.3, sca
     return cs[:, new].contiguous(), counts
 
 
+CONFIG3_DIMS = (20_000, 10_000, 5_000, 200)
+
+
 def served_stream(count, seed, rate=200.0, als_frac=0.7, ranks=(16, 32, 64), nnz_range=(50_000, 20_000_000),
-                  dim_range=(100, 50_000), orders=(3, 4, 5), apr_rank=8):
+                  dims=CONFIG3_DIMS, model_rank=8):
     """The served request stream: Poisson arrivals at `rate` per second;
-    each request CP-ALS (probability als_frac; uniform coordinates, values
-    uniform (0, 1]) or CP-APR (Poisson counts from a rank-`apr_rank`
-    Gamma(0.3, 1) Kruskal model); order uniform over `orders`, dimensions
-    log-uniform in dim_range, nnz log-uniform in nnz_range, rank uniform
-    over `ranks`.  Returns [(arrival_s, kind, dims, nnz, rank, seed), ...]."""
+    each request is CP-ALS (probability als_frac) or CP-APR on a tensor
+    generated as the CP-APR benchmark tensor is: `dims` (4-mode 20,000 x
+    10,000 x 5,000 x 200), Poisson counts from a rank-`model_rank`
+    Gamma(0.3, 1) Kruskal model (poisson_kruskal_torch) with a count total
+    log-uniform in nnz_range; CP-ALS requests decompose the counts as FP32
+    values.  Rank uniform over `ranks`.
+    Returns [(arrival_s, kind, dims, total_counts, rank, seed), ...]."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for k in range(count):
         t += rng.exponential(1.0 / rate)
         kind = "als" if rng.random() < als_frac else "apr"
-        nm = int(rng.choice(orders))
-        dims = tuple(int(round(np.exp(rng.uniform(np.log(dim_range[0]), np.log(dim_range[1]))))) for _ in range(nm))
         nnz = int(round(np.exp(rng.uniform(np.log(nnz_range[0]), np.log(nnz_range[1])))))
-        out.append((t, kind, dims, nnz, int(rng.choice(ranks)), int(rng.integers(1, 2**31))))
+        out.append((t, kind, tuple(int(d) for d in dims), nnz, int(rng.choice(ranks)), int(rng.integers(1, 2**31))))
     return out

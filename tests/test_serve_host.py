@@ -54,7 +54,7 @@ def test_served_stream_shape():
     nnz = np.array([x[3] for x in s])
     assert nnz.min() >= 50_000 and nnz.max() <= 20_000_000
     assert set(x[4] for x in s) == {16, 32, 64}
-    assert set(len(x[2]) for x in s) == {3, 4, 5}
+    assert all(x[2] == (20_000, 10_000, 5_000, 200) for x in s)
     assert synth.served_stream(10, 3) == s[:10]
 
 
