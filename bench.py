@@ -253,6 +253,21 @@ def cpu_baseline(args):
 
 # ------------------------------------------------------------ arms
 
+def rank_seed(base, rank):
+    """Seed of rank `rank`'s replica (weak scaling: every rank its own data)."""
+    return base + 7919 * rank
+
+
+def max_over_ranks(value, dist=None, device="cpu"):
+    """The job time of a replicated run: the slowest rank's (all-reduce MAX)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -320,7 +335,7 @@ def run_altob(args):
     stream = torch.cuda.current_stream(dev)
 
     # per-rank data: replicas of the workload with rank-dependent seeds (weak scaling)
-    cidx, vals, nnz = zipf_tensor_torch(DIMS, args.draws, ZIPF_S, SEED + 7919 * rank, dev)
+    cidx, vals, nnz = zipf_tensor_torch(DIMS, args.draws, ZIPF_S, rank_seed(SEED, rank), dev)
     at = ab.create_alto_device(3, np.array(DIMS, np.uint64), nnz, cidx, vals, nprtn=1024, lit_bits=128,
                                val_dtype="f32", stream=stream)
     del cidx, vals
@@ -365,10 +380,7 @@ def run_altob(args):
         dist.barrier()
     ms = t0.elapsed_time(t1)
     clocks = clk.stop()
-    if dist:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
     value = ws * nnz * 3 / (ms_step / 1e3) / 1e9
 
