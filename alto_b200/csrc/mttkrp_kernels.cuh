@@ -65,6 +65,16 @@ __device__ __forceinline__ void vload_plain(const FT* p, FT* x)
 }
 
 template <typename FT, int VEC>
+__device__ __forceinline__ void vload_stream(const FT* p, FT* x)
+{
+    typedef typename VecT<FT, VEC>::T V;
+    V v = __ldcs(reinterpret_cast<const V*>(p));
+    const FT* f = reinterpret_cast<const FT*>(&v);
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) x[e] = f[e];
+}
+
+template <typename FT, int VEC>
 __device__ __forceinline__ void vstore_zero(FT* p)
 {
     typedef typename VecT<FT, VEC>::T V;
@@ -419,6 +429,12 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 
 constexpr int GT_TILE = 1024;
 constexpr int GT_IPT = GT_TILE / MT_THREADS;
+// Streaming (evict-first) loads for data read once per launch (the key/value
+// stream, precomputed Khatri-Rao rows), so L2 keeps the gathered factor rows.
+__device__ __forceinline__ float ldcs_val(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ double ldcs_val(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ u32 ldcs_val(const u32* p) { return __ldcs(reinterpret_cast<const unsigned int*>(p)); }
+
 // Nonzeros a lane group takes per step in the run phase of the grouped kernels.
 #ifndef GT_NZS
 #define GT_NZS 2
@@ -506,7 +522,10 @@ __device__ __forceinline__ void nz_row(const u32* w, const FT* const* Uo, const 
 #pragma unroll
         for (int ch = 0; ch < CH; ++ch) {
             const int r0 = ch * LPN * VEC + sub * VEC;
-            if (r0 < R) vload<FT, VEC>(row + r0, y[k][ch]);
+            if (r0 < R) {
+                if constexpr (NM == 1) vload_stream<FT, VEC>(row + r0, y[k][ch]);  // precomputed row, read once
+                else vload<FT, VEC>(row + r0, y[k][ch]);
+            }
         }
     }
 #pragma unroll
@@ -664,8 +683,13 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
         if (it < nvalid) {
             const u64 pos = a.perm ? (u64)a.perm[g] : g;
             posv[k] = pos;
-            lo[k] = a.key.klo[pos];
-            vv[k] = vals[pos];
+            if (!a.perm) {  // the stream is read once: keep L2 for factor rows
+                lo[k] = __ldcs(reinterpret_cast<const unsigned long long*>(a.key.klo) + pos);
+                vv[k] = ldcs_val(vals + pos);
+            } else {
+                lo[k] = a.key.klo[pos];
+                vv[k] = vals[pos];
+            }
         }
     }
     int slv[GT_IPT];
