@@ -435,6 +435,17 @@ __device__ __forceinline__ float ldcs_val(const float* p) { return __ldcs(p); }
 __device__ __forceinline__ double ldcs_val(const double* p) { return __ldcs(p); }
 __device__ __forceinline__ u32 ldcs_val(const u32* p) { return __ldcs(reinterpret_cast<const unsigned int*>(p)); }
 
+// L2 prefetch of one row (R elements).  Phase A of the precomputed-row Phi
+// kernel issues it for the rows phase B will read, so they arrive from DRAM
+// while the tile is being sorted (measured: +9 % on CP-APR; the factor-row
+// gathers of MTTKRP are mostly L2 hits and lose 7 % to the extra issue).
+template <typename FT>
+__device__ __forceinline__ void prefetch_row(const FT* p, int R)
+{
+    const char* c = reinterpret_cast<const char*>(p);
+    for (int off = 0; off < R * (int)sizeof(FT); off += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+
 // Nonzeros a lane group takes per step in the run phase of the grouped kernels.
 #ifndef GT_NZS
 #define GT_NZS 2
@@ -713,6 +724,8 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
                 trow = field(lo[k], hi, a.fld.pos[target], a.fld.mask[target]);
                 r[0] = trow;
                 r[1] = (u32)posv[k];
+                // the precomputed row comes from DRAM: start fetching it now
+                prefetch_row<FT>(Uo[0] + (size_t)posv[k] * R, R);
             } else {
 #pragma unroll
                 for (int m = 0; m < MM; ++m) {
