@@ -429,12 +429,38 @@ altob_status altob_mttkrp_sweep_host(altob_tensor* t, altob_dtype ftype, void* c
     const size_t fsz = ftype == ALTOB_F64 ? 8 : 4;
     void* d[ALTOB_MAX_MODES];
     altob_status s = upload_factors(t, h_factors, fsz, rank, d, st);
+    // In the last sweep, factor m is final once mode m is done: its copy back
+    // runs on a second stream while the later modes compute.
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev[ALTOB_MAX_MODES] = {nullptr};
+    if (s == ALTOB_OK && iters > 0) {
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) cs = nullptr;
+        for (int m = 0; cs && m < t->nmode; ++m)
+            if (cudaEventCreateWithFlags(&ev[m], cudaEventDisableTiming) != cudaSuccess) ev[m] = nullptr;
+    }
     for (int i = 0; i < iters && s == ALTOB_OK; ++i)
-        for (int m = 0; m < t->nmode && s == ALTOB_OK; ++m) s = mttkrp_device(t, m, ftype, d, rank, 1, algo, st);
+        for (int m = 0; m < t->nmode && s == ALTOB_OK; ++m) {
+            s = mttkrp_device(t, m, ftype, d, rank, 1, algo, st);
+            if (s == ALTOB_OK && i == iters - 1 && cs && ev[m]) {
+                cudaEventRecord(ev[m], st);
+                cudaStreamWaitEvent(cs, ev[m], 0);
+                cudaError_t e = cudaMemcpyAsync(h_factors[m], d[m], t->dims[m] * rank * fsz, cudaMemcpyDeviceToHost,
+                                                cs);
+                if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep copy-out: ") + cudaGetErrorString(e));
+            }
+        }
     for (int m = 0; m < t->nmode && s == ALTOB_OK; ++m) {
+        if (cs && ev[m] && iters > 0) continue;  // already copied on the second stream
         cudaError_t e = cudaMemcpyAsync(h_factors[m], d[m], t->dims[m] * rank * fsz, cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep copy-out: ") + cudaGetErrorString(e));
     }
+    if (cs) {
+        cudaError_t e = cudaStreamSynchronize(cs);
+        if (s == ALTOB_OK && e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep: ") + cudaGetErrorString(e));
+        cudaStreamDestroy(cs);
+    }
+    for (int m = 0; m < ALTOB_MAX_MODES; ++m)
+        if (ev[m]) cudaEventDestroy(ev[m]);
     cudaError_t e = cudaStreamSynchronize(st);
     if (s == ALTOB_OK && e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("sweep: ") + cudaGetErrorString(e));
     return s;
