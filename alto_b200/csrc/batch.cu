@@ -11,11 +11,12 @@
 //   tensor's active flag when |fit - prev| < epsilon or max_iters is reached.
 // Inactive tensors are skipped by every kernel, so a tensor's result equals
 // its stand-alone solve.  Iterations after the first are captured once as a
-// CUDA graph and replayed.  A shape class is (order 3 or other, lanes per
-// nonzero, elements per lane, value type); its slot count and lane layout are
-// picked by altob_batch_autotune.
+// CUDA graph and replayed.  A shape class is (order, lanes per nonzero,
+// elements per lane, chunks, nnz decade, whether a mode reads through oidx);
+// its row-slot count and lane layout are picked by altob_batch_autotune.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -803,7 +804,10 @@ struct BatchImpl : BatchBase {
             }
             ALTOB_CUDA(cudaStreamSynchronize(st));
         }
-        // shape classes: (order 3 | 4-5, lanes, elements per lane, chunks)
+        // shape classes: (order, lanes, elements per lane, chunks, nnz decade,
+        // low-reuse flag) -- ALTOB_BATCH_CLASS_NNZ=0 drops the last two
+        const char* cn = getenv("ALTOB_BATCH_CLASS_NNZ");
+        const bool by_nnz = !(cn && atoi(cn) == 0);
         std::map<std::string, ClassRun<FT>*> byk;
         for (int b = 0; b < n; ++b) {
             altob_tensor* t = ts[b];
@@ -815,6 +819,13 @@ struct BatchImpl : BatchBase {
             char k[128];
             snprintf(k, sizeof(k), "order=%d lanes=%d vec=%d chunks=%d", t->nmode, pl.lpn, pl.vec,
                      pl.ch);
+            if (by_nnz) {
+                bool low = false;
+                for (int m = 0; m < t->nmode; ++m) low = low || (fib_reuse(t, m) <= 4 && t->d_oidx[m]);
+                const int dec = t->nnz < 100000 ? 4 : t->nnz < 1000000 ? 5 : 6;
+                const size_t l = strlen(k);
+                snprintf(k + l, sizeof(k) - l, " nnz=1e%d%s", dec, low ? " low-reuse" : "");
+            }
             auto it = byk.find(k);
             if (it == byk.end()) {
                 auto c = std::make_unique<ClassRun<FT>>();

@@ -246,8 +246,9 @@ ALTOB_API altob_status altob_batch_create(altob_tensor* const* tensors, int coun
                                           void* const* const* d_factors,
                                           void* const* d_lambda, int fit_capacity,
                                           void* stream, altob_batch** out);
-/* Picks, per shape class (order, lanes per nonzero, elements per
- * lane), the row-slot count and lane layout of the batched MTTKRP by timing
+/* Picks, per shape class (order, lanes per nonzero (from the rank),
+ * elements per lane, nnz decade, low fiber reuse), the row-slot count and
+ * lane layout of the batched MTTKRP by timing
  * every candidate on that class; leaves the factors unchanged.  Choices are
  * remembered per class for the rest of the process and applied to later
  * batches at creation; force = 0 tunes only classes without one. */
