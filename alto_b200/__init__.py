@@ -106,6 +106,7 @@ SIGNATURES = {
     "altob_cpd_als_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _d, _dp, C.POINTER(_i), _vp]),
     "altob_cp_apr_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _i, _d, _d, _d, _d, _i, _dp, _vp]),
     "altob_kruskal_random_init": (_i, [_i, _u64p, _u64, C.c_uint, _i, _vp, _vp]),
+    "altob_pseudo_inverse": (_i, [_vp, _i, _i, _u64, _vp, _u64, _i, C.POINTER(_i), _vp]),
     "altob_batch_create": (_i, [_vp, _i, _u64p, _i, _vp, _vp, _i, _vp, C.POINTER(_vp)]),
     "altob_batch_autotune": (_i, [_vp, _i, _vp]),
     "altob_batch_cpd_als": (_i, [_vp, _i, _d, _dp, C.POINTER(_i), _i, _vp]),
@@ -438,6 +439,19 @@ def cpd_alto(at: AltoTensor, M: KruskalModel, max_iters: int, epsilon: float, st
         _check(lib().altob_cpd_als(at.handle, ft, _ptr_array(ptrs), _dev_ptr(M.lam), M.rank, int(max_iters),
                                    float(epsilon), fits.ctypes.data_as(_dp), C.byref(it), _stream_ptr(stream)))
     return fits[:it.value]
+
+
+def pseudo_inverse(grams, mode, U, stream=None):
+    """pseudo_inverse (include/cpd.hpp:546-646) on the device: U <- U V^-1
+    (Cholesky) or U V^+ with V the Hadamard product of the Grams of every
+    mode but `mode`.  grams: CUDA FP64 tensor (nmode, R, R); U: CUDA tensor
+    (rows, R), updated in place.  Returns True when the pseudo-inverse was
+    used."""
+    used = C.c_int(0)
+    _check(lib().altob_pseudo_inverse(_dev_ptr(grams), int(grams.shape[0]), int(mode), int(U.shape[1]),
+                                      _dev_ptr(U), int(U.shape[0]), _ftype_of([U]), C.byref(used),
+                                      _stream_ptr(stream)))
+    return bool(used.value)
 
 
 def cp_apr_alto(at: AltoTensor, M: KruskalModel, max_iters: int, max_inner_iters: int, epsilon=1e-5,

@@ -423,7 +423,7 @@ struct BatchImpl : BatchBase {
 
     size_t smem_solve() const { return (size_t)2 * maxR * maxR * sizeof(double); }
     static size_t smem_apply(int R) { return (size_t)(R * R + R) * sizeof(double); }
-    static size_t smem_gram(int R) { return (size_t)(GR_ROWS * R + R) * sizeof(double); }
+    static size_t smem_gram(int R) { return (size_t)(GR_ELEMS + 2 * R) * sizeof(double); }
 
     // row kernels of mode j, one launch per rank class
     void launch_apply(int j, int nk, cudaStream_t st)

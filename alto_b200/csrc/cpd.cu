@@ -10,6 +10,7 @@
 // |fit - prev| < epsilon stopping rule.
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "dense.cuh"
@@ -107,6 +108,38 @@ altob_status check_model(const altob_tensor* t, altob_dtype ft, void* const* dU,
 }  // namespace altob
 
 using namespace altob;
+
+extern "C" altob_status altob_pseudo_inverse(const double* d_grams, int nmode, int mode, uint64_t rank, void* d_U,
+                                             uint64_t rows, altob_dtype ftype, int* used_pinv, void* stream)
+{
+    if (!d_grams || !d_U) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (nmode < 2 || nmode > ALTOB_MAX_MODES || mode < 0 || mode >= nmode) return fail(ALTOB_ERR_ARG, "bad mode");
+    if (ftype != ALTOB_F64 && ftype != ALTOB_F32) return fail(ALTOB_ERR_ARG, "dtype must be F64 or F32");
+    if (rank < 1) return fail(ALTOB_ERR_ARG, "rank must be >= 1");
+    if (rank > (u64)SOLVE_MAX_RANK) return fail(ALTOB_ERR_UNSUPPORTED, "rank above 112");
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
+    const int R = (int)rank;
+    double* W = nullptr;
+    ALTOB_TRY(dmalloc_t(&W, (size_t)R * R + 1));
+    int* info = (int*)(W + (size_t)R * R);
+    altob_status s = ALTOB_OK;
+    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
+    if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(e));
+    if (s == ALTOB_OK) s = solve_setup(d_grams, nmode, mode, R, W, info, st);
+    if (s == ALTOB_OK)
+        s = ftype == ALTOB_F64 ? apply_w<double>((double*)d_U, rows, R, W, NORM_NONE, nullptr, st)
+                               : apply_w<float>((float*)d_U, rows, R, W, NORM_NONE, nullptr, st);
+    int used = 0;
+    if (s == ALTOB_OK) {
+        e = cudaMemcpyAsync(&used, info, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = fail(ALTOB_ERR_CUDA, std::string("pseudo_inverse: ") + cudaGetErrorString(e));
+    }
+    dfree(W);
+    if (used_pinv) *used_pinv = used;
+    return s;
+}
 
 extern "C" altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype, void* const* d_factors, void* d_lambda,
                                       uint64_t rank, int max_iters, double epsilon, double* fits, int* iters,

@@ -17,16 +17,8 @@ altob_status gram(const FT* U, u64 I, int R, double* G, const double* div, FT* U
     ALTOB_CUDA(cudaMemsetAsync(G, 0, (size_t)R * R * sizeof(double), st));
     if (M) ALTOB_CUDA(cudaMemsetAsync(inner, 0, (size_t)R * sizeof(double), st));
     if (I == 0) return ALTOB_OK;
-    size_t smem = (size_t)(GR_ROWS * R + R) * sizeof(double);
-    const int g = dn_grid(I, 4 * GR_ROWS);
-    static std::atomic<int> configured{0};
-    if (smem > 48 * 1024 && !configured.load()) {
-        ALTOB_CUDA(cudaFuncSetAttribute(k_gram<FT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)((GR_ROWS * 128 + 128) * sizeof(double))));
-        ALTOB_CUDA(cudaFuncSetAttribute(k_gram<FT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)((GR_ROWS * 128 + 128) * sizeof(double))));
-        configured.store(1);
-    }
+    size_t smem = (size_t)(GR_ELEMS + 2 * R) * sizeof(double);  // < 48 KB for R <= 128
+    const int g = dn_grid(I, 2 * (GR_ELEMS / R));
     if (R <= GR_SMALL) k_gram<FT, 1><<<g, DN_THREADS, smem, st>>>(U, I, R, G, div, Uout, M, inner);
     else k_gram<FT, 3><<<g, DN_THREADS, smem, st>>>(U, I, R, G, div, Uout, M, inner);
     ALTOB_LAUNCH_CHECK();

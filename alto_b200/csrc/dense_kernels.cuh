@@ -27,10 +27,12 @@ static int dn_grid(u64 work, u64 per_block)
 // is given; X is written back to Uout when given; inner[r] += sum_i X[i,r] *
 // M[i,r] when M is given (cpd_fit_alto's inner product, cpd.hpp:207-213).
 // 4x4 register tiles of the lower triangle; rows of a staged chunk are split
-// across thread groups when there are fewer tiles than threads.
+// across thread groups when there are fewer tiles than threads.  A chunk holds
+// GR_ELEMS elements whatever the rank (GR_ELEMS / R rows), so small ranks
+// still keep GR_LD loads in flight per thread between barriers.
 
 constexpr int GR_TB = 4;
-constexpr int GR_ROWS = 64;
+constexpr int GR_ELEMS = 4096;
 constexpr int GR_LD = 8;      // staged elements in flight per thread
 constexpr int GR_SMALL = 88;  // R <= 88: at most 253 tiles, one per thread
 
@@ -40,9 +42,11 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
                                           const FT* __restrict__ M, double* __restrict__ inner, u64 bx, u64 nbx)
 {
     extern __shared__ double gsm[];
-    double* s = gsm;                 // GR_ROWS x R
-    double* si = gsm + GR_ROWS * R;  // R (inner partial)
+    double* s = gsm;                   // GR_ELEMS: rows x R
+    double* si = gsm + GR_ELEMS;       // R (inner partial)
+    double* sdiv = si + R;             // R (divisors)
     const int tid = threadIdx.x;
+    const int rows = GR_ELEMS / R;     // rows per chunk
     const int T = (R + GR_TB - 1) / GR_TB;
     const int NT = T * (T + 1) / 2;
     const int groups = NT >= DN_THREADS ? 1 : DN_THREADS / NT;
@@ -61,8 +65,11 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
 #pragma unroll
         for (int e = 0; e < GR_TB * GR_TB; ++e) acc[k][e] = 0.0;
     }
-    if (M) {
-        for (int r = tid; r < R; r += DN_THREADS) si[r] = 0.0;
+    if (M || div) {
+        for (int r = tid; r < R; r += DN_THREADS) {
+            si[r] = 0.0;
+            sdiv[r] = div ? div[r] : 1.0;
+        }
         __syncthreads();
     }
     // element e of a chunk sits in column (e mod R); for R dividing the
@@ -70,11 +77,11 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
     const bool fixed_col = DN_THREADS % R == 0;
     const int col_step = DN_THREADS % R;
     double pin = 0.0;
-    const u64 nchunks = (I + GR_ROWS - 1) / GR_ROWS;
+    const u64 nchunks = (I + rows - 1) / rows;
     for (u64 ch = bx; ch < nchunks; ch += nbx) {
-        const u64 r0 = ch * GR_ROWS;
-        const int nrows = (int)min((u64)GR_ROWS, I - r0);
-        const int tot = GR_ROWS * R, valid = nrows * R;
+        const u64 r0 = ch * rows;
+        const int nrows = (int)min((u64)rows, I - r0);
+        const int tot = rows * R, valid = nrows * R;
         const u64 base = r0 * (u64)R;  // a chunk is contiguous in memory
         __syncthreads();
         int col = tid % R;
@@ -93,7 +100,7 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
                     double x = (double)v[q];
                     if (e < valid) {
                         if (div) {
-                            x = x / div[col];
+                            x = x / sdiv[col];
                             if (Uout) Uout[base + e] = (FT)x;
                             x = (double)(FT)x;
                         }
@@ -162,6 +169,9 @@ __global__ void __launch_bounds__(DN_THREADS) k_gram(const FT* __restrict__ U, u
 }
 
 
+constexpr int JAC_MAX_PAIRS = (SOLVE_MAX_RANK + 1) / 2;
+constexpr int JAC_SWEEPS = 40;
+
 __device__ __forceinline__ void solve_body(const double* __restrict__ G, int nmode, int target, int R,
                                            double* __restrict__ W, int* __restrict__ info)
 {
@@ -169,7 +179,6 @@ __device__ __forceinline__ void solve_body(const double* __restrict__ G, int nmo
     double* A = ssm;          // R x R
     double* B = ssm + R * R;  // R x R
     __shared__ int ok;
-    __shared__ double cs[2];
     const int tid = threadIdx.x;
     for (int e = tid; e < R * R; e += DN_THREADS) {
         const int a = e / R, b = e - a * R;
@@ -222,60 +231,99 @@ __device__ __forceinline__ void solve_body(const double* __restrict__ G, int nmo
         }
         return;
     }
-    // ---- pseudo-inverse fallback: A = V (symmetric), B = eigenvectors
+    // ---- pseudo-inverse fallback: A = V (symmetric), B = eigenvectors.
+    // Two-sided Jacobi with the round-robin (tournament) ordering: each step
+    // rotates n/2 disjoint index pairs at once (n = R rounded up to even; the
+    // extra index is a dummy), n-1 steps make a sweep.  Sweeps stop when the
+    // off-diagonal mass is below 1e-26 of the total (eigenvectors to ~1e-13),
+    // at most JAC_SWEEPS of them.
     for (int e = tid; e < R * R; e += DN_THREADS) {
         const int a = e / R, b = e - a * R;
         A[e] = a >= b ? B[e] : B[b * R + a];
     }
     __syncthreads();
     for (int e = tid; e < R * R; e += DN_THREADS) B[e] = (e / R == e % R) ? 1.0 : 0.0;
+    const int n = (R + 1) & ~1, half = n / 2;
+    __shared__ double jc[JAC_MAX_PAIRS], js[JAC_MAX_PAIRS];
+    __shared__ int jp[JAC_MAX_PAIRS], jq[JAC_MAX_PAIRS];
+    __shared__ double red[2 * (DN_THREADS / 32)];
     __syncthreads();
-    for (int sweep = 0; sweep < 60; ++sweep) {
-        // convergence test
+    for (int sweep = 0; sweep < JAC_SWEEPS; ++sweep) {
+        // convergence test: block sums of squares (off-diagonal, total)
+        double off = 0.0, tot = 0.0;
+        for (int e = tid; e < R * R; e += DN_THREADS) {
+            const double x = A[e] * A[e];
+            tot += x;
+            if (e / R != e % R) off += x;
+        }
+        for (int o = 16; o; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if ((tid & 31) == 0) {
+            red[2 * (tid >> 5)] = off;
+            red[2 * (tid >> 5) + 1] = tot;
+        }
+        __syncthreads();
         if (tid == 0) {
-            double off = 0.0, tot = 0.0;
-            for (int e = 0; e < R * R; ++e) {
-                tot += A[e] * A[e];
-                if (e / R != e % R) off += A[e] * A[e];
+            double o2 = 0.0, t2 = 0.0;
+            for (int w = 0; w < DN_THREADS / 32; ++w) {
+                o2 += red[2 * w];
+                t2 += red[2 * w + 1];
             }
-            ok = off <= 1e-30 * tot;
+            ok = o2 <= 1e-26 * t2;
         }
         __syncthreads();
         if (ok) break;
-        for (int p = 0; p < R; ++p)
-            for (int q = p + 1; q < R; ++q) {
-                if (tid == 0) {
+        for (int step = 0; step < n - 1; ++step) {
+            // pair i: positions i and n-1-i of the arrangement [0, rotating 1..n-1]
+            for (int i = tid; i < half; i += DN_THREADS) {
+                const int a = i == 0 ? 0 : ((i - 1 + step) % (n - 1)) + 1;
+                const int bpos = n - 1 - i;
+                const int b = ((bpos - 1 + step) % (n - 1)) + 1;
+                const int p = a < b ? a : b, q = a < b ? b : a;
+                double c = 1.0, sn = 0.0;
+                if (q < R) {
                     const double apq = A[p * R + q];
-                    double c = 1.0, s = 0.0;
                     if (apq != 0.0) {
                         const double th = (A[q * R + q] - A[p * R + p]) / (2.0 * apq);
                         const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
                         c = 1.0 / sqrt(t * t + 1.0);
-                        s = t * c;
-                    }
-                    cs[0] = c;
-                    cs[1] = s;
-                }
-                __syncthreads();
-                const double c = cs[0], s = cs[1];
-                if (s != 0.0) {
-                    for (int k = tid; k < R; k += DN_THREADS) {
-                        const double akp = A[k * R + p], akq = A[k * R + q];
-                        A[k * R + p] = c * akp - s * akq;
-                        A[k * R + q] = s * akp + c * akq;
-                    }
-                    __syncthreads();
-                    for (int k = tid; k < R; k += DN_THREADS) {
-                        const double apk = A[p * R + k], aqk = A[q * R + k];
-                        A[p * R + k] = c * apk - s * aqk;
-                        A[q * R + k] = s * apk + c * aqk;
-                        const double vkp = B[k * R + p], vkq = B[k * R + q];
-                        B[k * R + p] = c * vkp - s * vkq;
-                        B[k * R + q] = s * vkp + c * vkq;
+                        sn = t * c;
                     }
                 }
-                __syncthreads();
+                jp[i] = p;
+                jq[i] = q;
+                jc[i] = c;
+                js[i] = sn;
             }
+            __syncthreads();
+            // columns p, q of A for every pair
+            for (int w = tid; w < half * R; w += DN_THREADS) {
+                const int i = w / R, k = w - i * R;
+                const int p = jp[i], q = jq[i];
+                if (q >= R || js[i] == 0.0) continue;
+                const double c = jc[i], sn = js[i];
+                const double akp = A[k * R + p], akq = A[k * R + q];
+                A[k * R + p] = c * akp - sn * akq;
+                A[k * R + q] = sn * akp + c * akq;
+            }
+            __syncthreads();
+            // rows p, q of A and columns p, q of the eigenvectors
+            for (int w = tid; w < half * R; w += DN_THREADS) {
+                const int i = w / R, k = w - i * R;
+                const int p = jp[i], q = jq[i];
+                if (q >= R || js[i] == 0.0) continue;
+                const double c = jc[i], sn = js[i];
+                const double apk = A[p * R + k], aqk = A[q * R + k];
+                A[p * R + k] = c * apk - sn * aqk;
+                A[q * R + k] = sn * apk + c * aqk;
+                const double vkp = B[k * R + p], vkq = B[k * R + q];
+                B[k * R + p] = c * vkp - sn * vkq;
+                B[k * R + q] = sn * vkp + c * vkq;
+            }
+            __syncthreads();
+        }
     }
     __syncthreads();
     double emax = 0.0;

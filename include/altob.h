@@ -163,6 +163,18 @@ ALTOB_API altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype,
                            uint64_t rank, int max_iters, double epsilon,
                            double* fits, int* iters, void* stream);
 
+/* Replaces pseudo_inverse (cpd.hpp:546-646): U <- U V^-1 with V the
+ * Hadamard product of the Grams of every mode but `mode` (d_grams: nmode
+ * R x R FP64 matrices, lower triangles used), by Cholesky when V is positive
+ * definite, else by V's pseudo-inverse (Jacobi eigendecomposition,
+ * eigenvalues below R * eps * max|lambda| dropped; the reference falls back
+ * to GELSY, the same minimum-norm solution).  d_U: rows x rank (ftype), in
+ * place.  *used_pinv (host, may be NULL) = 1 when the pseudo-inverse was
+ * used.  Synchronous. */
+ALTOB_API altob_status altob_pseudo_inverse(const double* d_grams, int nmode, int mode,
+                                            uint64_t rank, void* d_U, uint64_t rows,
+                                            altob_dtype ftype, int* used_pinv, void* stream);
+
 /* cpd_alto's own calling convention: the model (factors, lambda) in HOST
  * memory, copied to the device, solved, and copied back.  Synchronous. */
 ALTOB_API altob_status altob_cpd_als_host(altob_tensor* t, altob_dtype ftype,

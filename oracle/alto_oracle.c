@@ -525,7 +525,7 @@ static void jacobi_eig(double* A, double* V, int n)
 
 /* U <- U * V^{-1} with V = Hadamard of the Grams of the other modes.
  * Cholesky (lower) when V is positive definite, else pseudo-inverse. */
-static void pseudo_inverse(double** G, int nmode, int mode, double* U, u64 rows, u64 R)
+static int pseudo_inverse(double** G, int nmode, int mode, double* U, u64 rows, u64 R)
 {
     double* V = (double*)malloc(R * R * sizeof(double));
     for (u64 k = 0; k < R * R; ++k) V[k] = 1.0;
@@ -589,6 +589,16 @@ static void pseudo_inverse(double** G, int nmode, int mode, double* U, u64 rows,
         free(A); free(E); free(P);
     }
     free(x); free(L); free(V);
+    return !ok;
+}
+
+/* pseudo_inverse on Grams given as one nmode x R x R array; returns 1 when
+ * the pseudo-inverse (not the Cholesky solve) was used. */
+int orc_pseudo_inverse(const double* grams, int nmode, int mode, double* U, uint64_t rows, uint64_t R)
+{
+    double* G[8];
+    for (int m = 0; m < nmode; ++m) G[m] = (double*)(grams + (size_t)m * R * R);
+    return pseudo_inverse(G, nmode, mode, U, rows, R);
 }
 
 /* cpd_fit_alto (include/cpd.hpp:189-271). */

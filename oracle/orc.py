@@ -75,6 +75,8 @@ class Oracle:
         L.orc_loglik.restype = C.c_double
         L.orc_loglik.argtypes = [C.c_void_p, C.c_void_p, _f64p, C.c_uint64, C.c_double]
         L.orc_gram.argtypes = [_f64p, C.c_uint64, C.c_uint64, _f64p]
+        L.orc_pseudo_inverse.restype = C.c_int
+        L.orc_pseudo_inverse.argtypes = [_f64p, C.c_int, C.c_int, _f64p, C.c_uint64, C.c_uint64]
         self.L = L
 
     # -- encoding --
@@ -86,6 +88,14 @@ class Oracle:
         if rc != 0:
             raise ValueError(f"orc_create failed rc={rc}")
         return OracleTensor(self, h, dims, nnz, nprtn)
+
+    def pseudo_inverse(self, grams, mode, U):
+        """U <- U V^-1 (or V^+), V = Hadamard of the Grams but `mode`; returns
+        (U, used_pseudo_inverse)."""
+        grams = np.ascontiguousarray(grams, dtype=np.float64)
+        U = np.ascontiguousarray(U, dtype=np.float64).copy()
+        used = self.L.orc_pseudo_inverse(_p(grams, _f64p), grams.shape[0], mode, _p(U, _f64p), U.shape[0], U.shape[1])
+        return U, bool(used)
 
     def random_init(self, dims, rank, seed):
         dims = np.ascontiguousarray(dims, dtype=np.uint64)

@@ -1,6 +1,8 @@
 """CP-ALS and CP-APR on the GPU against fixtures written by the reference
 and against the oracle.  Fit and log-likelihood tolerance: 1e-4 (FP32
 model against the FP64 reference); FP64 runs are held much tighter."""
+import time
+
 import numpy as np
 import pytest
 
@@ -140,3 +142,51 @@ def test_gpu_phi_and_loglik_match_oracle(oracle):
     np.testing.assert_allclose(got, want, rtol=1e-12)
     assert rel_fro(dU[0].cpu().numpy(), oU[0]) < 1e-13
     np.testing.assert_allclose(dl.cpu().numpy(), olam, rtol=1e-12)
+
+
+def _grams(Us):
+    return np.stack([u.T @ u for u in Us])
+
+
+@pytest.mark.parametrize("R", [8, 37, 64])
+def test_gpu_pseudo_inverse_cholesky_matches_oracle(oracle, R):
+    """pseudo_inverse (cpd.hpp:546-646) with a positive definite V."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(R)
+    Us = [rng.random((d, R)) for d in (300, 200, 150)]
+    G = _grams(Us)
+    U = rng.random((500, R))
+    want, used_o = oracle.pseudo_inverse(G, 1, U)
+    dU = torch.from_numpy(U.copy()).cuda()
+    used = ab.pseudo_inverse(torch.from_numpy(G).cuda(), 1, dU)
+    assert not used and not used_o
+    assert rel_fro(dU.cpu().numpy(), want) < 1e-10
+
+
+@pytest.mark.parametrize("R", [6, 33, 64, 112])
+def test_gpu_pseudo_inverse_fallback_matches_oracle(oracle, R):
+    """A singular V (two equal columns in every other factor, integer entries
+    so that the Cholesky pivot is exactly 0 on every machine) takes the
+    pseudo-inverse path on both sides; the results agree."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(100 + R)
+    Us = []
+    for d in (40, 30, 25):
+        u = rng.integers(0, 3, size=(d, R)).astype(np.float64)
+        u[:, 0] = 0.0
+        u[0, 0] = 1.0
+        u[:, 1] = u[:, 0]
+        Us.append(u)
+    G = _grams(Us)
+    U = rng.random((200, R))
+    want, used_o = oracle.pseudo_inverse(G, 0, U)
+    dU = torch.from_numpy(U.copy()).cuda()
+    t0 = time.perf_counter()
+    used = ab.pseudo_inverse(torch.from_numpy(G).cuda(), 0, dU)
+    dt = time.perf_counter() - t0
+    assert used and used_o
+    assert rel_fro(dU.cpu().numpy(), want) < 1e-9
+    assert dt < 1.0  # parallel Jacobi: milliseconds, not a serial sweep per rotation
+    dU32 = torch.from_numpy(U.astype(np.float32)).cuda()
+    assert ab.pseudo_inverse(torch.from_numpy(G).cuda(), 0, dU32)
+    assert rel_fro(dU32.cpu().numpy(), want) < 1e-5
