@@ -41,12 +41,13 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
                                           const double* __restrict__ div, FT* __restrict__ Uout,
                                           const FT* __restrict__ M, double* __restrict__ inner, u64 bx, u64 nbx)
 {
-    extern __shared__ double gsm[];
-    double* s = gsm;                   // GR_ELEMS: rows x R
+    extern __shared__ __align__(16) double gsm[];
+    const int RS = (R + 3) & ~3;       // row stride in shared memory (zero padding)
+    const int rows = GR_ELEMS / RS;    // rows per chunk
+    double* s = gsm;                   // rows x RS (<= GR_ELEMS)
     double* si = gsm + GR_ELEMS;       // R (inner partial)
     double* sdiv = si + R;             // R (divisors)
     const int tid = threadIdx.x;
-    const int rows = GR_ELEMS / R;     // rows per chunk
     const int T = (R + GR_TB - 1) / GR_TB;
     const int NT = T * (T + 1) / 2;
     const int groups = NT >= DN_THREADS ? 1 : DN_THREADS / NT;
@@ -65,17 +66,17 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
 #pragma unroll
         for (int e = 0; e < GR_TB * GR_TB; ++e) acc[k][e] = 0.0;
     }
-    if (M || div) {
-        for (int r = tid; r < R; r += DN_THREADS) {
-            si[r] = 0.0;
-            sdiv[r] = div ? div[r] : 1.0;
-        }
-        __syncthreads();
+    for (int r = tid; r < R; r += DN_THREADS) {
+        si[r] = 0.0;
+        sdiv[r] = div ? div[r] : 1.0;
     }
+    if (RS != R)  // padding columns stay zero for every chunk
+        for (int e = tid; e < rows * (RS - R); e += DN_THREADS) s[(e / (RS - R)) * RS + R + e % (RS - R)] = 0.0;
+    __syncthreads();
     // element e of a chunk sits in column (e mod R); for R dividing the
     // block size that column is the same for every element of a thread
     const bool fixed_col = DN_THREADS % R == 0;
-    const int col_step = DN_THREADS % R;
+    const int col_step = DN_THREADS % R, row_step = DN_THREADS / R;
     double pin = 0.0;
     const u64 nchunks = (I + rows - 1) / rows;
     for (u64 ch = bx; ch < nchunks; ch += nbx) {
@@ -84,7 +85,7 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
         const int tot = rows * R, valid = nrows * R;
         const u64 base = r0 * (u64)R;  // a chunk is contiguous in memory
         __syncthreads();
-        int col = tid % R;
+        int col = tid % R, row = tid / R;
         for (int e0 = 0; e0 < tot; e0 += GR_LD * DN_THREADS) {
             FT v[GR_LD], mv[GR_LD];
 #pragma unroll
@@ -109,10 +110,14 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
                             else atomicAdd(&si[col], x * (double)mv[q]);
                         }
                     }
-                    s[e] = x;
+                    s[row * RS + col] = x;
                 }
                 col += col_step;
-                if (col >= R) col -= R;
+                row += row_step;
+                if (col >= R) {
+                    col -= R;
+                    ++row;
+                }
             }
         }
         __syncthreads();
@@ -122,13 +127,21 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
             if (ta[k] < 0) continue;
             const int a0 = ta[k] * GR_TB, b0 = tb[k] * GR_TB;
             for (int row = grp; row < nrows; row += groups) {
-                const double* sr = s + row * R;
+                const double* sr = s + row * RS;
+                // RS and the tile offsets are multiples of 4: 16-byte aligned pairs
+                const double2 a01 = *reinterpret_cast<const double2*>(sr + a0);
+                const double2 a23 = *reinterpret_cast<const double2*>(sr + a0 + 2);
+                const double2 b01 = *reinterpret_cast<const double2*>(sr + b0);
+                const double2 b23 = *reinterpret_cast<const double2*>(sr + b0 + 2);
                 double xa[GR_TB], xb[GR_TB];
-#pragma unroll
-                for (int q = 0; q < GR_TB; ++q) {
-                    xa[q] = a0 + q < R ? sr[a0 + q] : 0.0;
-                    xb[q] = b0 + q < R ? sr[b0 + q] : 0.0;
-                }
+                xa[0] = a01.x;
+                xa[1] = a01.y;
+                xa[2] = a23.x;
+                xa[3] = a23.y;
+                xb[0] = b01.x;
+                xb[1] = b01.y;
+                xb[2] = b23.x;
+                xb[3] = b23.y;
 #pragma unroll
                 for (int p = 0; p < GR_TB; ++p)
 #pragma unroll
