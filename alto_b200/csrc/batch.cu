@@ -264,6 +264,50 @@ struct ClassRun {
     }
 };
 
+// Classes that share a kernel template (order, lanes, elements per lane,
+// chunks, value type) after tuning run in one launch per mode; each tensor
+// keeps its class's row-slot count (the slot table is laid out for the
+// largest one).
+template <typename FT>
+struct LaunchGroup {
+    int nm = 0;
+    altob_dtype vdt = ALTOB_F32;
+    int lpn = 32, vec = 1, ch = 4;
+    int hmax = 0;
+    unsigned gridx = 1;
+    size_t smem = 0;
+    int count[ALTOB_MAX_MODES] = {0};
+    TiledArgs<FT>* d_args[ALTOB_MAX_MODES] = {nullptr};
+    u64* d_prefix[ALTOB_MAX_MODES] = {nullptr};
+    int* d_bid[ALTOB_MAX_MODES] = {nullptr};
+    u64 total_tiles[ALTOB_MAX_MODES] = {0};
+
+    TiledCfg cfg(unsigned gx) const
+    {
+        TiledCfg c;
+        c.lpn = lpn;
+        c.vec = vec;
+        c.ch = ch;
+        c.phi = 0;
+        c.grouped = 1;
+        c.grid = dim3(gx);
+        c.smem = smem;
+        return c;
+    }
+    void free_args()
+    {
+        for (int j = 0; j < ALTOB_MAX_MODES; ++j) {
+            dfree(d_args[j]);
+            dfree(d_prefix[j]);
+            dfree(d_bid[j]);
+            d_args[j] = nullptr;
+            d_prefix[j] = nullptr;
+            d_bid[j] = nullptr;
+            total_tiles[j] = 0;
+        }
+    }
+};
+
 struct BatchBase {
     virtual ~BatchBase() {}
     virtual altob_status autotune(int force, cudaStream_t st) = 0;
@@ -284,6 +328,7 @@ struct BatchImpl : BatchBase {
     int nlist[ALTOB_MAX_MODES] = {0};
     void* d_scratch = nullptr;
     std::vector<std::unique_ptr<ClassRun<FT>>> classes;
+    std::vector<std::unique_ptr<LaunchGroup<FT>>> groups;
     cudaStream_t cap_stream = nullptr;  // graph capture (never the legacy stream)
     cudaGraphExec_t gexec = nullptr;
     double g_eps = -1.0;
@@ -321,6 +366,7 @@ struct BatchImpl : BatchBase {
         }
         dfree(d_scratch);
         for (auto& c : classes) c->free_args();
+        for (auto& g : groups) g->free_args();
     }
 
     void drop_graph()
@@ -329,63 +375,137 @@ struct BatchImpl : BatchBase {
         gexec = nullptr;
     }
 
+    altob_status launch_mt(int nm, altob_dtype vdt, const BatchTiles<FT>& bt, const TiledCfg& cfg, cudaStream_t st,
+                           int* bps)
+    {
+        if (vdt == ALTOB_U32) return launch_batch<FT, u32>(bt, nm, cfg, st, bps);
+        return launch_batch<FT, FT>(bt, nm, cfg, st, bps);
+    }
     altob_status launch_mt(const ClassRun<FT>& c, const BatchTiles<FT>& bt, const TiledCfg& cfg, cudaStream_t st,
                            int* bps)
     {
-        if (c.vdt == ALTOB_U32) return launch_batch<FT, u32>(bt, c.nm, cfg, st, bps);
-        return launch_batch<FT, FT>(bt, c.nm, cfg, st, bps);
+        return launch_mt(c.nm, c.vdt, bt, cfg, st, bps);
+    }
+
+    // MTTKRP arguments of tensor b for target mode j with `hslots` row slots.
+    TiledArgs<FT> make_args(int b, int j, int hslots) const
+    {
+        altob_tensor* t = ts[b];
+        TiledArgs<FT> a;
+        memset(&a, 0, sizeof(a));
+        a.key = key_src(t);
+        a.vals = t->d_vals;
+        // low fiber reuse: read in the target mode's order (oidx), as the
+        // reference's op_sched dispatch does (alto.hpp:637-664)
+        a.perm = (fib_reuse(t, j) <= 4 && t->d_oidx[j]) ? t->d_oidx[j] : nullptr;
+        a.nnz = t->nnz;
+        a.ntiles = (t->nnz + GT_TILE - 1) / GT_TILE;
+        a.nmode = t->nmode;
+        a.target = j;
+        a.R = hdesc[b].R;
+        a.tile = GT_TILE;
+        a.hslots = hslots;
+        a.eps = FT(0);
+        for (int m = 0; m < t->nmode; ++m) a.U[m] = hdesc[b].U[m];
+        a.out = hdesc[b].U[j];
+        a.fld = t->fld;
+        return a;
+    }
+
+    // Uploads per-mode tables for (tensor, slots) members; returns counts.
+    altob_status upload_tables(const std::vector<std::pair<int, int>>& mem, TiledArgs<FT>** d_args, u64** d_prefix,
+                               int** d_bid, u64* total_tiles, int* count, cudaStream_t st)
+    {
+        for (int j = 0; j < maxN; ++j) {
+            std::vector<TiledArgs<FT>> args;
+            std::vector<u64> prefix;
+            std::vector<int> bid;
+            u64 tiles = 0;
+            for (const auto& m : mem) {
+                if (ts[m.first]->nmode <= j) continue;
+                args.push_back(make_args(m.first, j, m.second));
+                prefix.push_back(tiles);
+                bid.push_back(m.first);
+                tiles += args.back().ntiles;
+            }
+            prefix.push_back(tiles);
+            count[j] = (int)args.size();
+            total_tiles[j] = tiles;
+            if (args.empty()) continue;
+            ALTOB_TRY(dmalloc_t(&d_args[j], args.size()));
+            ALTOB_TRY(dmalloc_t(&d_prefix[j], prefix.size()));
+            ALTOB_TRY(dmalloc_t(&d_bid[j], bid.size()));
+            ALTOB_CUDA(cudaMemcpyAsync(d_args[j], args.data(), args.size() * sizeof(TiledArgs<FT>),
+                                       cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(d_prefix[j], prefix.data(), prefix.size() * sizeof(u64),
+                                       cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaMemcpyAsync(d_bid[j], bid.data(), bid.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            ALTOB_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+        }
+        return ALTOB_OK;
+    }
+
+    // Launch groups from the classes' current choices.
+    altob_status rebuild_groups(cudaStream_t st)
+    {
+        drop_graph();
+        for (auto& g : groups) g->free_args();
+        groups.clear();
+        std::map<std::string, std::vector<ClassRun<FT>*>> by;
+        for (auto& c : classes) {
+            char k[96];
+            snprintf(k, sizeof(k), "%d/%d/%d/%d/%d", c->nm, (int)c->vdt, c->lpn, c->vec, c->ch);
+            by[k].push_back(c.get());
+        }
+        for (auto& kv : by) {
+            auto g = std::make_unique<LaunchGroup<FT>>();
+            const ClassRun<FT>& c0 = *kv.second[0];
+            g->nm = c0.nm;
+            g->vdt = c0.vdt;
+            g->lpn = c0.lpn;
+            g->vec = c0.vec;
+            g->ch = c0.ch;
+            std::vector<std::pair<int, int>> mem;
+            for (ClassRun<FT>* c : kv.second) {
+                g->hmax = std::max(g->hmax, c->hslots);
+                for (int b : c->members) mem.push_back({b, c->hslots});
+            }
+            g->smem = grouped_smem(g->hmax, g->nm ? g->nm : ALTOB_MAX_MODES, sizeof(FT));
+            ALTOB_TRY(upload_tables(mem, g->d_args, g->d_prefix, g->d_bid, g->total_tiles, g->count, st));
+            BatchTiles<FT> bt;
+            memset(&bt, 0, sizeof(bt));
+            bt.hslots = g->hmax;
+            int bps = 0;
+            ALTOB_TRY(launch_mt(g->nm, g->vdt, bt, g->cfg(0), st, &bps));
+            if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "batched MTTKRP kernel does not fit on an SM");
+            g->gridx = (unsigned)(bps * num_sms());
+            groups.push_back(std::move(g));
+        }
+        return ALTOB_OK;
+    }
+
+    altob_status mttkrp_group(LaunchGroup<FT>& g, int j, cudaStream_t st)
+    {
+        if (!g.d_args[j] || g.total_tiles[j] == 0) return ALTOB_OK;
+        BatchTiles<FT> bt;
+        bt.args = g.d_args[j];
+        bt.tile_prefix = g.d_prefix[j];
+        bt.bid = g.d_bid[j];
+        bt.active = d_active;
+        bt.ntensors = g.count[j];
+        bt.hslots = g.hmax;
+        bt.total_tiles = g.total_tiles[j];
+        const unsigned gx = (unsigned)std::max<u64>(1, std::min<u64>(g.total_tiles[j], g.gridx));
+        return launch_mt(g.nm, g.vdt, bt, g.cfg(gx), st, nullptr);
     }
 
     // Per-mode argument tables of a class for its current slot count.
     altob_status build_class_args(ClassRun<FT>& c, cudaStream_t st)
     {
         c.free_args();
-        for (int j = 0; j < maxN; ++j) {
-            std::vector<TiledArgs<FT>> args;
-            std::vector<u64> prefix;
-            std::vector<int> bid;
-            u64 tiles = 0;
-            for (int b : c.members) {
-                altob_tensor* t = ts[b];
-                if (t->nmode <= j) continue;
-                TiledArgs<FT> a;
-                memset(&a, 0, sizeof(a));
-                a.key = key_src(t);
-                a.vals = t->d_vals;
-                // low fiber reuse: read in the target mode's order (oidx), as
-                // the reference's op_sched dispatch does (alto.hpp:637-664)
-                a.perm = (fib_reuse(t, j) <= 4 && t->d_oidx[j]) ? t->d_oidx[j] : nullptr;
-                a.nnz = t->nnz;
-                a.ntiles = (t->nnz + GT_TILE - 1) / GT_TILE;
-                a.nmode = t->nmode;
-                a.target = j;
-                a.R = hdesc[b].R;
-                a.tile = GT_TILE;
-                a.hslots = c.hslots;
-                a.eps = FT(0);
-                for (int m = 0; m < t->nmode; ++m) a.U[m] = hdesc[b].U[m];
-                a.out = hdesc[b].U[j];
-                a.fld = t->fld;
-                args.push_back(a);
-                prefix.push_back(tiles);
-                bid.push_back(b);
-                tiles += a.ntiles;
-            }
-            prefix.push_back(tiles);
-            c.mode_count[j] = (int)args.size();
-            c.total_tiles[j] = tiles;
-            if (args.empty()) continue;
-            ALTOB_TRY(dmalloc_t(&c.d_args[j], args.size()));
-            ALTOB_TRY(dmalloc_t(&c.d_prefix[j], prefix.size()));
-            ALTOB_TRY(dmalloc_t(&c.d_bid[j], bid.size()));
-            ALTOB_CUDA(cudaMemcpyAsync(c.d_args[j], args.data(), args.size() * sizeof(TiledArgs<FT>),
-                                       cudaMemcpyHostToDevice, st));
-            ALTOB_CUDA(cudaMemcpyAsync(c.d_prefix[j], prefix.data(), prefix.size() * sizeof(u64),
-                                       cudaMemcpyHostToDevice, st));
-            ALTOB_CUDA(cudaMemcpyAsync(c.d_bid[j], bid.data(), bid.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        }
-        ALTOB_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
-        return ALTOB_OK;
+        std::vector<std::pair<int, int>> mem;
+        for (int b : c.members) mem.push_back({b, c.hslots});
+        return upload_tables(mem, c.d_args, c.d_prefix, c.d_bid, c.total_tiles, c.mode_count, st);
     }
 
     // slot count and lane layout of a class -> argument tables and grid
@@ -481,9 +601,9 @@ struct BatchImpl : BatchBase {
             const int* L = d_list[j];
             const BlkMap els = {L, d_elpre[j], n};
             k_b_zero<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
-            for (auto& c : classes) {
-                ALTOB_TRY(mttkrp_class(*c, j, st));
-                launches += (c->d_args[j] && c->total_tiles[j]) ? 1 : 0;
+            for (auto& g : groups) {
+                ALTOB_TRY(mttkrp_group(*g, j, st));
+                launches += (g->d_args[j] && g->total_tiles[j]) ? 1 : 0;
             }
             launches += 5 + 2 * row_launches(j);
             k_b_copym<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
@@ -660,6 +780,7 @@ struct BatchImpl : BatchBase {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         ALTOB_CUDA(cudaGetLastError());
+        if (s == ALTOB_OK) s = rebuild_groups(st);
         ALTOB_CUDA(cudaStreamSynchronize(st));
         return s;
     }
@@ -667,8 +788,9 @@ struct BatchImpl : BatchBase {
     void describe(std::string* out) const override
     {
         char line[320];
-        snprintf(line, sizeof(line), "tensors=%d classes=%zu max_modes=%d max_rank=%d launches_per_iteration=%d\n",
-                 count, classes.size(), maxN, maxR, launches_per_iter);
+        snprintf(line, sizeof(line),
+                 "tensors=%d classes=%zu launch_groups=%zu max_modes=%d max_rank=%d launches_per_iteration=%d\n",
+                 count, classes.size(), groups.size(), maxN, maxR, launches_per_iter);
         *out += line;
         for (auto& c : classes) {
             snprintf(line, sizeof(line), "class %s: tensors=%zu slots=%d lanes=%d chunks=%d tuned_ms=%.4f\n",
@@ -850,6 +972,7 @@ struct BatchImpl : BatchBase {
                 ALTOB_TRY(set_choice(*c, c->hslots, c->lpn, c->ch, st));
             }
         }
+        ALTOB_TRY(rebuild_groups(st));
         ALTOB_CUDA(cudaStreamSynchronize(st));
         return ALTOB_OK;
     }
