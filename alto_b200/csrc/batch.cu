@@ -330,6 +330,9 @@ struct BatchImpl : BatchBase {
     std::vector<std::unique_ptr<ClassRun<FT>>> classes;
     std::vector<std::unique_ptr<LaunchGroup<FT>>> groups;
     cudaStream_t cap_stream = nullptr;  // graph capture (never the legacy stream)
+    static constexpr int NFORK = 4;     // streams the launch groups of a mode spread over
+    cudaStream_t fork_st[NFORK] = {nullptr};
+    cudaEvent_t fork_ev = nullptr, join_ev[NFORK] = {nullptr};
     cudaGraphExec_t gexec = nullptr;
     double g_eps = -1.0;
     int g_iters = -1;
@@ -353,6 +356,11 @@ struct BatchImpl : BatchBase {
         StreamScope scope(0);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        for (int i = 0; i < NFORK; ++i) {
+            if (fork_st[i]) cudaStreamDestroy(fork_st[i]);
+            if (join_ev[i]) cudaEventDestroy(join_ev[i]);
+        }
+        if (fork_ev) cudaEventDestroy(fork_ev);
         dfree(d_desc);
         dfree(d_active);
         dfree(d_iters);
@@ -601,9 +609,22 @@ struct BatchImpl : BatchBase {
             const int* L = d_list[j];
             const BlkMap els = {L, d_elpre[j], n};
             k_b_zero<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
-            for (auto& g : groups) {
-                ALTOB_TRY(mttkrp_group(*g, j, st));
-                launches += (g->d_args[j] && g->total_tiles[j]) ? 1 : 0;
+            // the launch groups of mode j are independent: spread them over
+            // forked streams so one group's last wave overlaps the others
+            ALTOB_CUDA(cudaEventRecord(fork_ev, st));
+            int used = 0;
+            for (size_t gi = 0; gi < groups.size(); ++gi) {
+                LaunchGroup<FT>& g = *groups[gi];
+                if (!g.d_args[j] || g.total_tiles[j] == 0) continue;
+                cudaStream_t fs = fork_st[used % NFORK];
+                if (used < NFORK) ALTOB_CUDA(cudaStreamWaitEvent(fs, fork_ev, 0));
+                ALTOB_TRY(mttkrp_group(g, j, fs));
+                ++used;
+                ++launches;
+            }
+            for (int i = 0; i < std::min(used, NFORK); ++i) {
+                ALTOB_CUDA(cudaEventRecord(join_ev[i], fork_st[i]));
+                ALTOB_CUDA(cudaStreamWaitEvent(st, join_ev[i], 0));
             }
             launches += 5 + 2 * row_launches(j);
             k_b_copym<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
@@ -973,6 +994,11 @@ struct BatchImpl : BatchBase {
             }
         }
         ALTOB_TRY(rebuild_groups(st));
+        for (int i = 0; i < NFORK; ++i) {
+            ALTOB_CUDA(cudaStreamCreateWithFlags(&fork_st[i], cudaStreamNonBlocking));
+            ALTOB_CUDA(cudaEventCreateWithFlags(&join_ev[i], cudaEventDisableTiming));
+        }
+        ALTOB_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
         ALTOB_CUDA(cudaStreamSynchronize(st));
         return ALTOB_OK;
     }
