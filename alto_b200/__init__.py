@@ -76,7 +76,7 @@ class Result(C.Structure):
 class ServerConfig(C.Structure):
     """altob_server_config (include/altob.h)."""
     _fields_ = [("hbm_budget", C.c_uint64), ("workers", C.c_int), ("max_batch", C.c_int), ("use_graph", C.c_int),
-                ("autotune", C.c_int), ("plain", C.c_int)]
+                ("autotune", C.c_int), ("plain", C.c_int), ("policy", C.c_int)]
 
 # name -> (restype, argtypes); the exported C ABI of include/altob.h
 _vp, _u64, _i, _d = C.c_void_p, C.c_uint64, C.c_int, C.c_double

@@ -71,8 +71,17 @@ struct Job {
     altob_request req;
     altob_result res;
     u64 fp = 0;
+    double est_s = 0.0;  // estimated device seconds (scheduling only)
     bool done = false;
 };
+
+// Work estimate of a request at an assumed 10 Gnnz/s of MTTKRP / Phi passes.
+static double est_seconds(const altob_request& r)
+{
+    double passes = (double)r.nmode * (double)r.max_iters;
+    if (r.kind == ALTOB_REQ_CP_APR) passes *= (double)std::max(1, r.max_inner);
+    return (double)r.nnz * passes / 1e10;
+}
 
 }  // namespace altob
 
@@ -97,23 +106,37 @@ struct altob_server {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
 
-    // Next group to run, or empty: the queue head if it fits, plus (CP-ALS)
-    // the queued CP-ALS requests behind it that fit.  Called with mu held.
-    std::vector<Job*> take()
+    // Next group to run, or empty: the first request by the policy (queue
+    // order, or least estimated work net of waiting time) if it fits, plus
+    // (CP-ALS) the queued CP-ALS requests that can share its batched solve.
+    // Called with mu held.
+    std::vector<Job*> take(int worker)
     {
         std::vector<Job*> g;
         if (queue.empty()) return g;
-        Job* h = queue.front();
+        auto pick = queue.begin();
+        if (cfg.policy == 1) {
+            const double t = now();
+            double best = 1e300;
+            for (auto it = queue.begin(); it != queue.end(); ++it) {
+                const double score = (*it)->est_s - (t - (*it)->res.t_submit);
+                if (score < best) {
+                    best = score;
+                    pick = it;
+                }
+            }
+        }
+        Job* h = *pick;
         if (h->fp > cfg.hbm_budget) {  // can never run
-            queue.pop_front();
+            queue.erase(pick);
             h->res.status = fail(ALTOB_ERR_NOMEM, "request footprint above the server's HBM budget");
             h->res.t_start = h->res.t_end = now();
             h->done = true;
             cv_done.notify_all();
-            return take();
+            return take(worker);
         }
         if (used + h->fp > cfg.hbm_budget) return g;
-        queue.pop_front();
+        queue.erase(pick);
         used += h->fp;
         g.push_back(h);
         if (h->req.kind == ALTOB_REQ_CPD_ALS && !cfg.plain) {
@@ -134,7 +157,7 @@ struct altob_server {
         return g;
     }
 
-    void worker_main()
+    void worker_main(int worker)
     {
         cudaSetDevice(device);
         cudaStream_t st = nullptr;
@@ -145,7 +168,7 @@ struct altob_server {
                 std::unique_lock<std::mutex> lk(mu);
                 for (;;) {
                     if (stop && queue.empty()) break;
-                    g = take();
+                    g = take(worker);
                     if (!g.empty()) break;
                     cv_work.wait(lk);
                 }
@@ -286,13 +309,14 @@ altob_status altob_server_create(const altob_server_config* cfg, altob_server** 
     if (cfg->workers < 1 || cfg->workers > 64) return fail(ALTOB_ERR_ARG, "workers must be 1..64");
     if (cfg->max_batch < 1) return fail(ALTOB_ERR_ARG, "max_batch must be >= 1");
     if (cfg->hbm_budget == 0) return fail(ALTOB_ERR_ARG, "HBM budget must be > 0");
+    if (cfg->policy != 0 && cfg->policy != 1) return fail(ALTOB_ERR_ARG, "policy must be 0 or 1");
     int dev = 0;
     ALTOB_CUDA(cudaGetDevice(&dev));
     altob_server* s = new altob_server();
     s->cfg = *cfg;
     s->device = dev;
     s->t0 = std::chrono::steady_clock::now();
-    for (int w = 0; w < cfg->workers; ++w) s->workers.emplace_back([s] { s->worker_main(); });
+    for (int w = 0; w < cfg->workers; ++w) s->workers.emplace_back([s, w] { s->worker_main(w); });
     *out = s;
     return ALTOB_OK;
 }
@@ -311,6 +335,7 @@ altob_status altob_server_submit(altob_server* s, const altob_request* r, uint64
     j->req = *r;
     memset(&j->res, 0, sizeof(j->res));
     j->fp = footprint(*r);
+    j->est_s = est_seconds(*r);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stop) {

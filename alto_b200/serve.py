@@ -25,9 +25,12 @@ ALS, APR = 0, 1
 
 
 class Server:
-    def __init__(self, hbm_budget_gb=150.0, workers=4, max_batch=32, use_graph=True, autotune=True, plain=False):
+    POLICIES = {"fifo": 0, "least_work": 1}
+
+    def __init__(self, hbm_budget_gb=150.0, workers=4, max_batch=32, use_graph=True, autotune=True, plain=False,
+                 policy="fifo"):
         cfg = ServerConfig(int(hbm_budget_gb * (1 << 30)), int(workers), int(max_batch), int(bool(use_graph)),
-                           int(bool(autotune)), int(bool(plain)))
+                           int(bool(autotune)), int(bool(plain)), self.POLICIES[policy])
         h = C.c_void_p()
         _check(lib().altob_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h.value

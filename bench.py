@@ -84,6 +84,7 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=60)
     p.add_argument("--serve-workers", type=int, default=4)
     p.add_argument("--serve-batch", type=int, default=32)
+    p.add_argument("--serve-policy", default="fifo", choices=["fifo", "least_work"])
     p.add_argument("--batch-count", type=int, default=512)
     p.add_argument("--batch-iters", type=int, default=25)
     p.add_argument("--no-baseline", action="store_true", help="batch: skip the one-at-a-time FP64 arm")
@@ -599,7 +600,8 @@ def run_serve(args):
         return out
 
     # served path; a short warm-up stream first tunes the shape classes
-    srv = serve.Server(hbm_budget_gb=150, workers=args.serve_workers, max_batch=args.serve_batch)
+    srv = serve.Server(hbm_budget_gb=150, workers=args.serve_workers, max_batch=args.serve_batch,
+                       policy=args.serve_policy)
     reqs = requests(ab.F32)
     nw = min(len(reqs), 12)
     serve.replay(srv, reqs[:nw], [0.0] * nw)
@@ -618,7 +620,7 @@ def run_serve(args):
     base = None
     agree = None
     if not args.no_baseline:
-        srv = serve.Server(hbm_budget_gb=150, workers=1, max_batch=1, plain=True)
+        srv = serve.Server(hbm_budget_gb=150, workers=1, max_batch=1, plain=True, policy="fifo")
         bres, bsumm = serve.replay(srv, requests(ab.F64), arrivals)
         srv.close()
         base = dict(bsumm, path="plain one-at-a-time FP64: altob_cpd_als / altob_cp_apr, one worker, no batching")
@@ -640,7 +642,8 @@ def run_serve(args):
             "config": {"workload": f"served_stream_{len(inputs)}req_200rps", "requests": len(inputs),
                        "als": sum(1 for x in inputs if x[0] == "als"), "apr": sum(1 for x in inputs if x[0] == "apr"),
                        "nnz_total": int(sum(int(x[3].shape[0]) for x in inputs)), "hbm_budget_gb": 150,
-                       "workers": args.serve_workers, "max_batch": args.serve_batch},
+                       "workers": args.serve_workers, "max_batch": args.serve_batch,
+                       "policy": args.serve_policy},
             "served": summ, "peak_admitted_bytes": peak, "baseline_fp64_one_at_a_time": base,
             "speedup_vs_fp64_one_at_a_time": (summ["solves_per_s"] / base["solves_per_s"]) if base else None,
             "agreement_vs_fp64": agree, "clocks": clocks}

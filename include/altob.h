@@ -282,7 +282,11 @@ ALTOB_API altob_status altob_batch_destroy(altob_batch* b);
  * batches run at once, each worker on its own CUDA stream.  A worker that
  * admits a CP-ALS request takes the queued CP-ALS requests behind it with
  * the same dtypes, iteration limit and tolerance (up to max_batch, within
- * the budget) into one altob_batch solve.  With plain = 1 every request runs
+ * the budget) into one altob_batch solve.  The request a free worker starts
+ * is the queue head (policy 0) or the one with the least estimated work
+ * (nonzeros x modes x iterations, x inner iterations for CP-APR, at an
+ * assumed 10 Gnnz/s) after subtracting the time it has waited (policy 1:
+ * short requests pass long ones, no request waits forever).  With plain = 1 every request runs
  * alone through altob_cpd_als / altob_cp_apr (no batching).  Factors are
  * initialised on the device from the request's seed, identically alone or in
  * a batch.  The request's COO arrays (device, as for altob_create_device)
@@ -324,6 +328,8 @@ typedef struct {
     int use_graph;       /* replay batched iterations from a CUDA graph */
     int autotune;        /* tune unseen shape classes on first use */
     int plain;           /* 1: no batching, altob_cpd_als per request */
+    int policy;          /* 0: arrival order; 1: least estimated work first, a
+                            request's estimate shrinking by 1 s per second waited */
 } altob_server_config;
 
 typedef struct altob_server altob_server;

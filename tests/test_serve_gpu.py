@@ -105,3 +105,27 @@ def test_admission_respects_budget():
     res, _ = _mix(items[:3], ab.F32, workers=2, max_batch=2, hbm_budget_gb=small / (1 << 30))
     for r, fp in zip(res, fps[:3]):
         assert (r["status"] == ab.ERR_NOMEM) == (fp > small)
+
+
+@pytest.mark.parametrize("policy", ["fifo", "least_work"])
+def test_admission_policy_order(policy):
+    """One worker, a long CP-APR request queued first and short CP-ALS
+    requests behind it: arrival order runs the long one first, least-work
+    order runs the short ones first; the results are the same either way."""
+    dims = (200, 150, 100, 40)
+    cidx, cnt = synth.poisson_kruskal_torch(dims, 8, 400_000, 77, "cuda")
+    small = [synth.uniform_coo_torch((60, 50, 40), 5_000, 80 + k, "cuda") for k in range(3)]
+    srv = serve.Server(workers=1, max_batch=1, policy=policy)
+    # hold the worker with a first request so that the rest queue up together
+    hold = srv.submit_apr(dims, cidx, cnt, 8, max_iters=3, tol=0.0, seed=1, max_inner=3)
+    big = srv.submit_apr(dims, cidx, cnt, 8, max_iters=8, tol=0.0, seed=2, max_inner=5)
+    ids = [srv.submit_als((60, 50, 40), c, v.float(), 8, max_iters=5, tol=0.0, seed=3 + k)
+           for k, (c, v) in enumerate(small)]
+    res = {i: srv.wait(i) for i in [hold, big] + ids}
+    srv.close()
+    assert all(r["status"] == 0 for r in res.values())
+    short_done = max(res[i]["t_end"] for i in ids)
+    if policy == "fifo":
+        assert res[big]["t_end"] <= min(res[i]["t_start"] for i in ids)
+    else:
+        assert short_done <= res[big]["t_start"]
