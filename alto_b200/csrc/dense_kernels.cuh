@@ -149,7 +149,23 @@ __device__ __forceinline__ void gram_body(const FT* __restrict__ U, u64 I, int R
             }
         }
     }
-    if (active) {
+    // row groups hold partial copies of the same tiles: sum them in shared
+    // memory (the staging buffer is free now) so each tile entry takes one
+    // global atomic per CTA
+    bool flush = active;
+    if (MAXT == 1 && groups > 1) {
+        __syncthreads();
+        if (active)
+#pragma unroll
+            for (int e = 0; e < GR_TB * GR_TB; ++e) s[tid * GR_TB * GR_TB + e] = acc[0][e];
+        __syncthreads();
+        flush = tid < NT;
+        if (flush)
+            for (int g = 1; g < groups; ++g)
+#pragma unroll
+                for (int e = 0; e < GR_TB * GR_TB; ++e) acc[0][e] += s[(g * NT + tid) * GR_TB * GR_TB + e];
+    }
+    if (flush) {
 #pragma unroll
         for (int k = 0; k < MAXT; ++k) {
             if (ta[k] < 0) continue;
