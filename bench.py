@@ -34,6 +34,11 @@ FP32 values), rank from {16, 32, 64}, tolerance 1e-4, at most 50 iterations,
 150 GB HBM budget; FP32 served path (concurrent workers, CP-ALS batching)
 beside the plain one-at-a-time FP64 path on the same stream.
 
+--workload cpals runs CP-ALS on the same large tensor (rank 32, 10
+iterations) with the FP32 model (FP64 Gram/solve/fit) and with the FP64 model
+on FP64 values from the same initial factors, and reports the time per
+iteration and the fit agreement.
+
 --workload apr runs CP-APR on the 4-mode count tensor 20,000 x 10,000 x 5,000
 x 200 (INT32 Poisson counts from a rank-10 Gamma(0.3, 1) Kruskal model, about
 50M distinct nonzeros), rank 16, FP32 model with FP64 KKT and
@@ -78,7 +83,7 @@ def parse():
     p.add_argument("--cpu-sample-draws", type=int, default=40_000_000)
     p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
     p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
-    p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch", "serve", "apr"])
+    p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch", "serve", "apr", "cpals"])
     p.add_argument("--apr-nnz", type=int, default=50_000_000, help="apr: target distinct nonzeros")
     p.add_argument("--apr-outer", type=int, default=50)
     p.add_argument("--serve-requests", type=int, default=60)
@@ -652,6 +657,64 @@ def run_serve(args):
     return 0
 
 
+def run_cpals(args):
+    """CP-ALS on the large skewed tensor (see the module docstring)."""
+    import torch
+    import alto_b200 as ab
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    iters = 10
+    cidx, vals, nnz = zipf_tensor_torch(DIMS, args.draws, ZIPF_S, rank_seed(SEED, rank), dev)
+    d = np.array(DIMS, np.uint64)
+    at32 = ab.create_alto_device(3, d, nnz, cidx, vals, nprtn=1024, lit_bits=128, val_dtype="f32")
+    at64 = None if args.no_baseline else ab.create_alto_device(3, d, nnz, cidx, vals.double(), nprtn=1024,
+                                                                lit_bits=128, val_dtype="f64")
+    del cidx, vals
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED)
+    init = [torch.rand(x, RANK, dtype=torch.float64, device=dev, generator=g) for x in DIMS]
+
+    def model(dt):
+        return ab.KruskalModel(list(DIMS), RANK, [u.to(dt).clone() for u in init],
+                               torch.ones(RANK, dtype=dt, device=dev))
+
+    ab.cpd_alto(at32, model(torch.float32), 1, 0.0)  # warm-up
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    clk = ClockSampler()
+    clk.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    f32 = ab.cpd_alto(at32, model(torch.float32), iters, 0.0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms32 = e0.elapsed_time(e1)
+    f64, ms64 = None, None
+    if at64 is not None:
+        e0.record(stream)
+        f64 = ab.cpd_alto(at64, model(torch.float64), iters, 0.0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+    line = {"metric": "cpals_ms_per_iteration", "value": ms32 / iters, "unit": "ms", "n_gpus": ws, "steps": iters,
+            "warmup": 1, "ms_per_step": ms32 / iters, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 Gram/solve/fit)", "data": "synthetic",
+            "config": {"workload": "cpals_zipf3_4.8Mx1.8Mx1.8M", "dims": list(DIMS), "nnz": nnz, "rank": RANK,
+                       "iterations": iters, "alto_bits": 65},
+            "mttkrp_gnnz_per_s_per_mode_in_solve": nnz * 3 * iters / (ms32 / 1e3) / 1e9,
+            "fits_fp32": list(map(float, f32)), "fits_fp64": list(map(float, f64)) if f64 is not None else None,
+            "fp64_ms_per_iteration": ms64 / iters if ms64 else None,
+            "fit_max_abs_diff_fp32_vs_fp64": float(np.max(np.abs(np.array(f32) - np.array(f64))))
+            if f64 is not None else None, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_apr(args):
     """CP-APR workload (see the module docstring)."""
     import torch
@@ -751,6 +814,8 @@ def main():
         return run_serve(args)
     if args.workload == "apr":
         return run_apr(args)
+    if args.workload == "cpals":
+        return run_cpals(args)
     return run_altob(args)
 
 
