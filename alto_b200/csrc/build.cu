@@ -67,6 +67,21 @@ altob_status tensor_scratch(altob_tensor* t, size_t bytes, void** out)
     return ALTOB_OK;
 }
 
+altob_status tensor_hotbuf(altob_tensor* t, size_t bytes, void** out)
+{
+    if (bytes > t->hotbuf_bytes) {
+        if (t->hotbuf) {
+            dfree(t->hotbuf);
+            t->hotbuf = nullptr;
+            t->hotbuf_bytes = 0;
+        }
+        ALTOB_TRY(dmalloc(&t->hotbuf, bytes));
+        t->hotbuf_bytes = bytes;
+    }
+    *out = t->hotbuf;
+    return ALTOB_OK;
+}
+
 int num_sms()
 {
     static int sms = 0;
@@ -944,6 +959,7 @@ altob_status altob_destroy(altob_tensor* t)
     dfree(t->d_vals);
     for (int n = 0; n < ALTOB_MAX_MODES; ++n) dfree(t->d_oidx[n]);
     dfree(t->scratch);
+    dfree(t->hotbuf);
     delete t;
     return ALTOB_OK;
 }

@@ -207,6 +207,9 @@ struct altob_tensor {
     // cached scratch (grown on demand, freed with the handle)
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // per-CTA hot-row accumulators of the grouped kernel (grown on demand)
+    void* hotbuf = nullptr;
+    size_t hotbuf_bytes = 0;
 };
 
 namespace altob {
@@ -245,6 +248,7 @@ void dfree(void* p);
 // Per-tensor scratch: returns a device buffer of at least `bytes`, reused
 // across calls on the same handle.
 altob_status tensor_scratch(altob_tensor* t, size_t bytes, void** out);
+altob_status tensor_hotbuf(altob_tensor* t, size_t bytes, void** out);
 
 int num_sms();
 

@@ -67,15 +67,31 @@ altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, 
         const int slots = env_int("ALTOB_GROUP_SLOTS", 2048);
         pl->hslots = cache ? std::max(32, std::min(floor_pow2(slots), 8192)) : 0;
         const int mm = t->nmode >= 3 ? t->nmode : ALTOB_MAX_MODES;
-        pl->smem = grouped_smem(pl->hslots, mm, fsz);
+        pl->hot = env_int("ALTOB_HOT_ROWS", 1) ? grouped_hot_slots((int)R, fsz) : 0;
+        pl->smem = grouped_smem(pl->hslots, mm, fsz, pl->hot, (int)R);
         return ALTOB_OK;
     }
+    pl->hot = 0;
     pl->tile = env_int("ALTOB_TILE", 1024);
     pl->tile = std::max(256, (pl->tile / 256) * 256);
     int cache_bytes = env_int("ALTOB_CACHE_BYTES", 32 * 1024);
     long long rows = (long long)cache_bytes / (long long)(R * fsz);
     pl->hslots = (cache && rows >= 16) ? std::min(floor_pow2(rows), 4096) : 0;
     pl->smem = tiled_smem(t->nmode, pl->tile, pl->hslots, (int)R, fsz);
+    return ALTOB_OK;
+}
+
+// Per-CTA hot-row accumulator regions for a launch of `grid` CTAs (none when
+// the kernel has no hot-row slots).
+template <typename FT>
+static altob_status set_hot_acc(altob_tensor* t, TiledArgs<FT>& a, unsigned grid, cudaStream_t st)
+{
+    (void)st;
+    a.hot_acc = nullptr;
+    if (!a.hot) return ALTOB_OK;
+    void* p = nullptr;
+    ALTOB_TRY(tensor_hotbuf(t, (size_t)grid * a.hot * a.R * sizeof(FT), &p));
+    a.hot_acc = (FT*)p;
     return ALTOB_OK;
 }
 
@@ -103,6 +119,7 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     for (int m = 0; m < t->nmode; ++m) a.U[m] = (const FT*)dU[m];
     a.out = (FT*)dout;
     a.fld = t->fld;
+    a.hot = pl.grouped ? pl.hot : 0;
     TiledCfg c;
     c.lpn = pl.lpn;
     c.vec = pl.vec;
@@ -116,6 +133,7 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "MTTKRP kernel does not fit on an SM");
     u64 cap = (u64)bps * num_sms();
     c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, cap)));
+    ALTOB_TRY(set_hot_acc(t, a, c.grid.x, st));
     return launch_tiled<FT, VT>(a, c, st, nullptr);
 }
 
@@ -326,6 +344,7 @@ static altob_status run_phi_pre_vt(altob_tensor* t, int mode, const void* dpi, c
     a.U[1] = (const FT*)dB;
     a.out = (FT*)dphi;
     a.fld = t->fld;
+    a.hot = env_int("ALTOB_HOT_ROWS", 1) ? grouped_hot_slots((int)R, sizeof(FT)) : 0;
     TiledCfg c;
     c.lpn = pl.lpn;
     c.vec = pl.vec;
@@ -333,13 +352,14 @@ static altob_status run_phi_pre_vt(altob_tensor* t, int mode, const void* dpi, c
     c.phi = 1;
     c.grouped = 1;
     c.pre = 1;
-    c.smem = grouped_smem(a.hslots, 2, sizeof(FT));
+    c.smem = grouped_smem(a.hslots, 2, sizeof(FT), a.hot, (int)R);
     c.grid = dim3(0);
     int bps = 0;
     ALTOB_TRY((launch_tiled<FT, VT>(a, c, st, &bps)));
     if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "Phi kernel does not fit on an SM");
     const u64 cap = (u64)bps * num_sms();
     c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, cap)));
+    ALTOB_TRY(set_hot_acc(t, a, c.grid.x, st));
     return launch_tiled<FT, VT>(a, c, st, nullptr);
 }
 

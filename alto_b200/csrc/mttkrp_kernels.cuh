@@ -163,6 +163,8 @@ struct TiledArgs {
     const FT* U[ALTOB_MAX_MODES];
     FT* out;
     Fields fld;
+    int hot;       // per-CTA hot-row slots (power of two; 0: none), grouped kernel only
+    FT* hot_acc;   // gridDim.x x hot x R accumulators, one private region per CTA
 };
 
 // Dynamic shared-memory bytes of k_tiled.
@@ -475,13 +477,36 @@ struct RecWords {
     static constexpr int n = (MM + (int)(sizeof(FT) / 4) + 3) & ~3;
 };
 
-inline size_t grouped_smem(int hslots, int mm, size_t fsz)
+inline size_t grouped_smem(int hslots, int mm, size_t fsz, int hot = 0, int R = 0)
 {
     const int rw = (mm + (int)(fsz / 4) + 3) & ~3;
     size_t b = (size_t)GT_TILE * rw * 4 * 2;  // records, then records in run order
     b += (size_t)hslots * 8;                  // tags + counts
     b += (size_t)GT_TILE * 4;                 // claimed-slot list
+    b += (size_t)hot * 4;                     // hot-row tags
+    (void)R;
     return b;
+}
+
+// Runs shorter than GT_HOT_MINRUN nonzeros skip the hot-row lookup (rows
+// that are hot fill long runs in a tile).
+#ifndef GT_HOT_MINRUN
+#define GT_HOT_MINRUN 8
+#endif
+
+// Hot-row cache of the grouped kernel: per CTA, `hot` direct-mapped rows
+// (row & (hot - 1), claimed first come, tags in shared memory) whose run sums
+// go to a region of global memory private to the CTA (L2-resident, no
+// contention) and reach the output once per CTA instead of once per tile.
+// Rows that many tiles touch (the head of a skewed mode) then take a few
+// hundred FP32 additions instead of one per tile, which keeps their rounding
+// error near the per-tile level.  16 KB per CTA; FP32 only.
+inline int grouped_hot_slots(int R, size_t fsz)
+{
+    if (fsz != 4 || R < 1) return 0;
+    int h = 1;
+    while (h * 2 <= 256 && (size_t)(h * 2) * R * fsz <= 16384) h *= 2;
+    return h >= 16 ? h : 0;
 }
 
 template <typename FT, int RW>
@@ -504,9 +529,45 @@ __device__ __forceinline__ FT rec_val(const u32* w)
     else return (FT)__longlong_as_double((long long)(((unsigned long long)w[MM + 1] << 32) | w[MM]));
 }
 
+struct GroupedSmem {
+    u32* rec;
+    u32* srec;
+    u32* tag;
+    u32* cnt;
+    u32* used;
+    u32* htag;   // hot-row tags (row + 1; 0 free)
+    u32* nused;
+    u32* ndirect;
+    u32* wsum;
+};
+
+// One run sum into its output row: into the CTA's hot-row slot when the row
+// holds (or can claim) it, else with vector atomics into the output.
 template <typename FT, int VEC, int CH, int LPN>
-__device__ __forceinline__ void flush_run(FT* out, u32 row, int R, int sub, FT (*racc)[VEC])
+__device__ __forceinline__ void flush_run(FT* out, const GroupedSmem& gs, int hot, FT* hot_acc, unsigned gmask,
+                                          u32 row, int R, int sub, FT (*racc)[VEC])
 {
+    if (hot) {
+        const u32 sl = row & (u32)(hot - 1);
+        u32 tg = 0;
+        if (sub == 0) {
+            tg = gs.htag[sl];
+            if (tg == 0u) {
+                const u32 old = atomicCAS(&gs.htag[sl], 0u, row + 1u);
+                tg = old == 0u ? row + 1u : old;
+            }
+        }
+        tg = __shfl_sync(gmask, tg, __ffs(gmask) - 1);
+        if (tg == row + 1u) {
+            FT* h = hot_acc + ((size_t)blockIdx.x * hot + sl) * R;
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) {
+                const int r0 = ch * LPN * VEC + sub * VEC;
+                if (r0 < R) gred<FT, VEC>(h + r0, racc[ch]);
+            }
+            return;
+        }
+    }
 #pragma unroll
     for (int ch = 0; ch < CH; ++ch) {
         const int r0 = ch * LPN * VEC + sub * VEC;
@@ -592,19 +653,9 @@ __device__ __forceinline__ void run_add(FT (*racc)[VEC], FT (*x)[VEC])
 
 // Shared-memory work areas of the grouped kernels (tags and counts must be
 // zero between tiles; grouped_tile leaves them zero).
-struct GroupedSmem {
-    u32* rec;
-    u32* srec;
-    u32* tag;
-    u32* cnt;
-    u32* used;
-    u32* nused;
-    u32* ndirect;
-    u32* wsum;
-};
 
 template <typename FT, int MM>
-__device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, int H, u32* statics)
+__device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, int H, u32* statics, int hot = 0)
 {
     constexpr int RW = RecWords<FT, MM>::n;
     GroupedSmem g;
@@ -613,6 +664,8 @@ __device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, in
     g.tag = g.srec + (size_t)GT_TILE * RW;
     g.cnt = g.tag + H;
     g.used = g.cnt + H;
+    g.htag = g.used + GT_TILE;
+    (void)hot;
     g.nused = statics;
     g.ndirect = statics + 1;
     g.wsum = statics + 2;
@@ -835,6 +888,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     __syncthreads();
     // ---- B: runs of equal output rows, one atomic per run
     u32 prow = 0xffffffffu;
+    int rlen = 0;  // nonzeros in the current run
     FT racc[CH][VEC];
 #pragma unroll
     for (int ch = 0; ch < CH; ++ch)
@@ -855,14 +909,16 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
 #pragma unroll
         for (int q = 0; q < GT_NZS; ++q) {
             if (w[q][0] != prow) {
-                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+                if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, gs, rlen >= GT_HOT_MINRUN ? a.hot : 0, a.hot_acc, gmask, prow, R, sub, racc);
                 prow = w[q][0];
+                rlen = 1;
 #pragma unroll
                 for (int ch = 0; ch < CH; ++ch)
 #pragma unroll
                     for (int e = 0; e < VEC; ++e) racc[ch][e] = x[q][ch][e];
             } else {
                 run_add<FT, VEC, CH>(racc, x[q]);
+                ++rlen;
             }
         }
     }
@@ -872,17 +928,19 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
         FT x0[CH][VEC];
         nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
         if (w0[0] != prow) {
-            if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+            if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, gs, rlen >= GT_HOT_MINRUN ? a.hot : 0, a.hot_acc, gmask, prow, R, sub, racc);
             prow = w0[0];
+            rlen = 1;
 #pragma unroll
             for (int ch = 0; ch < CH; ++ch)
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) racc[ch][e] = x0[ch][e];
         } else {
             run_add<FT, VEC, CH>(racc, x0);
+            ++rlen;
         }
     }
-    if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, prow, R, sub, racc);
+    if (prow != 0xffffffffu) flush_run<FT, VEC, CH, LPN>(a.out, gs, rlen >= GT_HOT_MINRUN ? a.hot : 0, a.hot_acc, gmask, prow, R, sub, racc);
     __syncthreads();
     // counts back to zero for the next tile (tags were cleared in A2)
     for (u32 e = tid; e < nu; e += MT_THREADS) cnt[used[e]] = 0;
@@ -899,10 +957,21 @@ __global__ void GT_BOUNDS k_grouped(TiledArgs<FT> a)
     constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 statics[2 + MT_WARPS];
-    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, a.hslots, statics);
-    grouped_init(gs, a.hslots);
+    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, a.hslots, statics, a.hot);
+    FT* hacc = a.hot ? a.hot_acc + (size_t)blockIdx.x * a.hot * a.R : nullptr;
+    for (int k = threadIdx.x; k < a.hot; k += MT_THREADS) gs.htag[k] = 0;
+    for (int k = threadIdx.x; k < a.hot * a.R; k += MT_THREADS) hacc[k] = FT(0);
+    grouped_init(gs, a.hslots);  // ends with a barrier: the zeroed region precedes every run flush
     for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x)
         grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(a, ti, gs);
+    if (a.hot) {  // the CTA's hot-row sums, once each (read from L2, where the atomics landed)
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.hot * a.R; k += MT_THREADS) {
+            const int sl = k / a.R;
+            const u32 tg = gs.htag[sl];
+            if (tg) atomicAdd(a.out + (size_t)(tg - 1u) * a.R + (k - sl * a.R), __ldcg(hacc + k));
+        }
+    }
 }
 
 // Batched form: the tiles of many tensors (one TiledArgs each, same shape

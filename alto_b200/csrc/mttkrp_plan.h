@@ -7,6 +7,7 @@ namespace altob {
 
 struct TiledPlan {
     int vec, lpn, ch, tile, hslots, grouped;
+    int hot;  // hot-row slots per CTA (grouped kernel, FP32)
     size_t smem;
 };
 

@@ -99,37 +99,9 @@ def parse():
 # ------------------------------------------------------------ data (torch)
 
 def zipf_tensor_torch(dims, draws, s, seed, device):
-    """Config-2 tensor generated on the device: inverse-CDF Zipf draws per
-    mode, duplicate coordinates merged by summing log-normal values."""
-    import torch
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    idx = []
-    for d in dims:
-        k = torch.arange(1, d + 1, dtype=torch.float64, device=device)
-        cdf = torch.cumsum(k.pow(-s), 0)
-        cdf /= cdf[-1].clone()
-        u = torch.rand(draws, dtype=torch.float64, device=device, generator=g)
-        i = torch.searchsorted(cdf, u, right=True).clamp_(max=d - 1)
-        idx.append(i)
-        del k, cdf, u
-    vals = torch.exp(torch.randn(draws, dtype=torch.float64, device=device, generator=g))
-    low = idx[1] * dims[2] + idx[2]
-    o1 = torch.sort(low, stable=True).indices
-    o2 = torch.sort(idx[0][o1], stable=True).indices
-    order = o1[o2]
-    del o1, o2
-    i0, lo, v = idx[0][order], low[order], vals[order]
-    del idx, low, vals, order
-    new = torch.ones_like(i0, dtype=torch.bool)
-    new[1:] = (i0[1:] != i0[:-1]) | (lo[1:] != lo[:-1])
-    seg = torch.cumsum(new.to(torch.int64), 0) - 1
-    nnz = int(seg[-1].item()) + 1
-    vs = torch.zeros(nnz, dtype=torch.float64, device=device).index_add_(0, seg, v)
-    keep = new.nonzero().squeeze(1)
-    i0, lo = i0[keep], lo[keep]
-    cidx = torch.stack([i0, lo // dims[2], lo % dims[2]]).contiguous()
-    return cidx, vs.to(torch.float32), nnz
+    """Config-2 tensor generated on the device (alto_b200.synth.zipf_tensor_torch)."""
+    from alto_b200 import synth
+    return synth.zipf_tensor_torch(dims, draws, s, seed, device)
 
 
 # ------------------------------------------------------------- clocks
