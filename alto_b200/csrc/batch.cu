@@ -4,9 +4,12 @@
 // Every tensor of the batch keeps its own device model and follows exactly
 // the per-tensor algorithm of cpd_alto (include/cpd.hpp:43-186, as in
 // cpd.cu), but each step runs for all tensors in one launch:
-//   zero U_j | MTTKRP (one launch per shape class) | copy of the last mode |
-//   prepare | R x R solve (one CTA per tensor) | row apply + column norms |
-//   lambda | Gram of the normalised factor  -- for every mode j --
+//   zero U_j | MTTKRP (one launch per shape class) | prepare |
+//   R x R solve (one CTA per tensor) | fused row update + column norms +
+//   Gram (+ fit inner product) | lambda, Gram scaling | U_j /= lambda
+//   -- for every mode j; rank classes above 64 keep the separate passes
+//   (copy of the last mode, row apply + column norms, lambda, Gram of the
+//   normalised factor) --
 //   then the fit, which also records the per-iteration fit and clears the
 //   tensor's active flag when |fit - prev| < epsilon or max_iters is reached.
 // Inactive tensors are skipped by every kernel, so a tensor's result equals
@@ -84,7 +87,7 @@ __global__ void k_b_copym(const BDesc<FT>* __restrict__ d, BlkMap map, const int
     const int b = blk_owner(map, &bx, &nbx);
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
-    if (j != t.nmode - 1) return;
+    if (j != t.nmode - 1 || t.R <= APPLY_GRAM_MAX_RANK) return;  // the fused pass reads M itself
     const u64 n = t.dims[j] * (u64)t.R;
     for (u64 e = (u64)bx * blockDim.x + threadIdx.x; e < n; e += (u64)nbx * blockDim.x) t.M[e] = t.U[j][e];
 }
@@ -127,13 +130,50 @@ __global__ void __launch_bounds__(DN_THREADS) k_b_apply(const BDesc<FT>* __restr
     apply_body<FT, LPR, CJ>(t.U[j], t.dims[j], t.R, t.W, nk, t.colacc, bx, nbx);
 }
 
+// fused row update + Gram of U_j (R <= 64, see apply_gram_body), one launch
+// per rank class
+template <typename FT, int MB>
+__global__ void __launch_bounds__(AG_THREADS) k_b_apply_gram(const BDesc<FT>* __restrict__ d, BlkMap map,
+                                                             const int* __restrict__ active, int j, int nk)
+{
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    const int R = t.R;
+    const int vec_ok = ((uintptr_t)t.U[j] & 15) == 0;
+    apply_gram_body<FT, MB>(t.U[j], t.dims[j], R, t.W, nk, t.colacc, t.G + (size_t)j * R * R,
+                            j == t.nmode - 1 ? t.inner : nullptr, vec_ok, bx, nbx);
+}
+
+// U_j /= lambda after the fused pass
+template <typename FT>
+__global__ void __launch_bounds__(DN_THREADS) k_b_div_cols(const BDesc<FT>* __restrict__ d, BlkMap map,
+                                                           const int* __restrict__ active, int j)
+{
+    int bx, nbx;
+    const int b = blk_owner(map, &bx, &nbx);
+    if (!active[b]) return;
+    const BDesc<FT>& t = d[b];
+    constexpr int V = 16 / sizeof(FT);
+    if (t.R % V == 0 && ((uintptr_t)t.U[j] & 15) == 0) div_cols_body<FT, V>(t.U[j], t.dims[j], t.R, t.lam, bx, nbx);
+    else div_cols_body<FT, 1>(t.U[j], t.dims[j], t.R, t.lam, bx, nbx);
+}
+
+// lambda from the column statistics; after the fused pass (R <= 64) also
+// G_j /= lambda lambda^T and the inner product /= lambda
 template <typename FT>
 __global__ void k_b_lambda(const BDesc<FT>* __restrict__ d, const int* __restrict__ list,
-                           const int* __restrict__ active, int nk)
+                           const int* __restrict__ active, int nk, int j)
 {
     const int b = list[blockIdx.x];
     if (!active[b]) return;
     const BDesc<FT>& t = d[b];
+    if (t.R <= APPLY_GRAM_MAX_RANK) {
+        lambda_finish_body(t.colacc, t.R, nk, t.lam, t.G + (size_t)j * t.R * t.R,
+                           j == t.nmode - 1 ? t.inner : nullptr);
+        return;
+    }
     for (int r = threadIdx.x; r < t.R; r += blockDim.x) t.lam[r] = nk == NORM_2 ? sqrt(t.colacc[r]) : t.colacc[r];
 }
 
@@ -553,11 +593,36 @@ struct BatchImpl : BatchBase {
     static size_t smem_apply(int R) { return (size_t)(R * R + R) * sizeof(double); }
     static size_t smem_gram(int R) { return (size_t)(GR_ELEMS + 2 * R) * sizeof(double); }
 
-    // row kernels of mode j, one launch per rank class
+    // fused row update + Gram of mode j for the rank classes up to 64
+    void launch_apply_gram(int j, int nk, cudaStream_t st)
+    {
+        for (int c = 0; c < NRANK_CLASSES; ++c) {
+            if (!ncl[j][c] || !fused_class(c)) continue;
+            const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
+            const int g = nrowblk[j][c];
+            switch (c) {
+            case 0: k_b_apply_gram<FT, 1><<<g, AG_THREADS, apply_gram_smem<1>(), st>>>(d_desc, m, d_active, j, nk); break;
+            case 1: k_b_apply_gram<FT, 2><<<g, AG_THREADS, apply_gram_smem<2>(), st>>>(d_desc, m, d_active, j, nk); break;
+            case 2: k_b_apply_gram<FT, 4><<<g, AG_THREADS, apply_gram_smem<4>(), st>>>(d_desc, m, d_active, j, nk); break;
+            default: k_b_apply_gram<FT, 8><<<g, AG_THREADS, apply_gram_smem<8>(), st>>>(d_desc, m, d_active, j, nk); break;
+            }
+        }
+    }
+    // U_j /= lambda for the fused rank classes (after k_b_lambda)
+    void launch_div_cols(int j, cudaStream_t st)
+    {
+        for (int c = 0; c < NRANK_CLASSES; ++c) {
+            if (!ncl[j][c] || !fused_class(c)) continue;
+            const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
+            k_b_div_cols<FT><<<nrowblk[j][c], DN_THREADS, cmaxR[c] * sizeof(double), st>>>(d_desc, m, d_active, j);
+        }
+    }
+    static bool fused_class(int c) { return c <= 3; }  // rank classes up to R = 64
+    // row kernels of mode j for the rank classes above 64, one launch per class
     void launch_apply(int j, int nk, cudaStream_t st)
     {
         for (int c = 0; c < NRANK_CLASSES; ++c) {
-            if (!ncl[j][c]) continue;
+            if (!ncl[j][c] || fused_class(c)) continue;
             const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
             const size_t sm = smem_apply(cmaxR[c]);
             const int g = nrowblk[j][c];
@@ -573,7 +638,7 @@ struct BatchImpl : BatchBase {
     void launch_gram(int j, int scaled, cudaStream_t st)
     {
         for (int c = 0; c < NRANK_CLASSES; ++c) {
-            if (!ncl[j][c]) continue;
+            if (!ncl[j][c] || (scaled && fused_class(c))) continue;
             const BlkMap m = {d_clist[j][c], d_rowpre[j][c], ncl[j][c]};
             const size_t sm = smem_gram(cmaxR[c]);
             const int g = nrowblk[j][c];
@@ -630,8 +695,10 @@ struct BatchImpl : BatchBase {
             k_b_copym<FT><<<nelblk[j], 256, 0, st>>>(d_desc, els, d_active, j);
             k_b_prep<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, j, nk);
             k_b_solve<FT><<<n, DN_THREADS, smem_solve(), st>>>(d_desc, L, d_active, j);
+            launch_apply_gram(j, nk, st);
             launch_apply(j, nk, st);
-            k_b_lambda<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, nk);
+            k_b_lambda<FT><<<n, 128, 0, st>>>(d_desc, L, d_active, nk, j);
+            launch_div_cols(j, st);
             launch_gram(j, 1, st);
             ALTOB_LAUNCH_CHECK();
         }

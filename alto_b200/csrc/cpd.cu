@@ -30,8 +30,13 @@ static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, in
 {
     const int N = t->nmode;
     const u64 IN = t->dims[N - 1];
+    // R <= 64: one fused pass (row update, statistics, Gram, inner product)
+    // and one division pass per mode instead of the row-apply and Gram passes;
+    // the fused pass reads the last mode's MTTKRP before overwriting it, so the
+    // copy of it for the fit is not needed
+    const bool fused = R <= APPLY_GRAM_MAX_RANK && env_int("ALTOB_FUSED_APPLY", 1);
     size_t nd = (size_t)N * R * R + (size_t)R * R + 3 * (size_t)R + 8;
-    size_t bytes = nd * sizeof(double) + 256 + IN * R * sizeof(FT) + 256;
+    size_t bytes = nd * sizeof(double) + 256 + (fused ? 0 : IN * R * sizeof(FT)) + 256;
     void* base = nullptr;
     ALTOB_TRY(tensor_scratch(t, bytes, &base));
     AlsScratch s;
@@ -67,6 +72,15 @@ static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, in
         const NormKind nk = i == 0 ? NORM_2 : NORM_MAX;
         for (int j = 0; j < N; ++j) {
             ALTOB_TRY(mttkrp_device(t, j, ft, (void* const*)U, (u64)R, 0, ALTOB_ALGO_AUTO, st));
+            if (fused) {
+                double* Gj = s.G + (size_t)j * R * R;
+                double* inner = j == N - 1 ? s.inner : nullptr;
+                ALTOB_TRY(solve_setup(s.G, N, j, R, s.W, s.info, st));
+                ALTOB_TRY(apply_gram<FT>(U[j], t->dims[j], R, s.W, nk, s.colacc, Gj, inner, st));
+                ALTOB_TRY(lambda_finish(s.colacc, R, nk, s.lam, Gj, inner, st));
+                ALTOB_TRY(normalize_cols<FT>(U[j], t->dims[j], R, s.lam, st));
+                continue;
+            }
             if (j == N - 1)
                 ALTOB_CUDA(cudaMemcpyAsync(s.M, U[j], IN * R * sizeof(FT), cudaMemcpyDeviceToDevice, st));
             ALTOB_TRY(solve_setup(s.G, N, j, R, s.W, s.info, st));

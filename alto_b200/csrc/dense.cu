@@ -89,6 +89,74 @@ altob_status apply_w(FT* U, u64 I, int R, const double* W, NormKind nk, double* 
     }
 }
 
+// ------------------------------------------- fused row update + Gram (R <= 64)
+
+template <typename FT, int MB>
+static altob_status launch_apply_gram(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, double* G,
+                                      double* inner, cudaStream_t st)
+{
+    static std::atomic<int> per_sm{0};  // resident blocks per SM (one value per instantiation)
+    if (per_sm.load() == 0) {
+        int n = 0;
+        ALTOB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_apply_gram<FT, MB>, AG_THREADS,
+                                                                 apply_gram_smem<MB>()));
+        per_sm.store(std::max(1, n));
+    }
+    const u64 groups = (I + 7) / 8;
+    const int per_block = AG_THREADS / 32 * 4;  // at least 4 row groups per warp
+    const u64 want = (groups + per_block - 1) / per_block;
+    const int grid = (int)std::max<u64>(1, std::min<u64>(want, (u64)num_sms() * per_sm.load()));
+    const int vec_ok = ((uintptr_t)U & 15) == 0;
+    k_apply_gram<FT, MB><<<grid, AG_THREADS, apply_gram_smem<MB>(), st>>>(U, I, R, W, (int)nk, colacc, G, inner,
+                                                                        vec_ok);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+template <typename FT>
+altob_status apply_gram(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, double* G, double* inner,
+                        cudaStream_t st)
+{
+    if (R > APPLY_GRAM_MAX_RANK) return fail(ALTOB_ERR_UNSUPPORTED, "rank above 64 in the fused row update");
+    if (nk == NORM_2) ALTOB_CUDA(cudaMemsetAsync(colacc, 0, (size_t)R * sizeof(double), st));
+    else if (nk == NORM_MAX) ALTOB_TRY(vec_fill(colacc, R, 1.0, st));
+    ALTOB_CUDA(cudaMemsetAsync(G, 0, (size_t)R * R * sizeof(double), st));
+    if (inner) ALTOB_CUDA(cudaMemsetAsync(inner, 0, (size_t)R * sizeof(double), st));
+    if (I == 0) return ALTOB_OK;
+    switch ((R + 7) / 8) {
+    case 1: return launch_apply_gram<FT, 1>(U, I, R, W, nk, colacc, G, inner, st);
+    case 2: return launch_apply_gram<FT, 2>(U, I, R, W, nk, colacc, G, inner, st);
+    case 3: return launch_apply_gram<FT, 3>(U, I, R, W, nk, colacc, G, inner, st);
+    case 4: return launch_apply_gram<FT, 4>(U, I, R, W, nk, colacc, G, inner, st);
+    case 5: return launch_apply_gram<FT, 5>(U, I, R, W, nk, colacc, G, inner, st);
+    case 6: return launch_apply_gram<FT, 6>(U, I, R, W, nk, colacc, G, inner, st);
+    case 7: return launch_apply_gram<FT, 7>(U, I, R, W, nk, colacc, G, inner, st);
+    default: return launch_apply_gram<FT, 8>(U, I, R, W, nk, colacc, G, inner, st);
+    }
+}
+
+altob_status lambda_finish(const double* colacc, int R, NormKind nk, double* lam, double* G, double* inner,
+                           cudaStream_t st)
+{
+    k_lambda_finish<<<1, DN_THREADS, 0, st>>>(colacc, R, (int)nk, lam, G, inner);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+template <typename FT>
+altob_status normalize_cols(FT* U, u64 I, int R, const double* lam, cudaStream_t st)
+{
+    if (I == 0) return ALTOB_OK;
+    constexpr int V = 16 / sizeof(FT);
+    const bool vec = R % V == 0 && ((uintptr_t)U & 15) == 0;
+    const u64 n = I * (u64)R;
+    const size_t smem = (size_t)R * sizeof(double);
+    if (vec) k_div_cols<FT, V><<<dn_grid(n / V, DN_THREADS * 4), DN_THREADS, smem, st>>>(U, I, R, lam);
+    else k_div_cols<FT, 1><<<dn_grid(n, DN_THREADS * 4), DN_THREADS, smem, st>>>(U, I, R, lam);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
 // ------------------------------------------------------------- small ops
 
 altob_status lambda_from(const double* colacc, int R, NormKind nk, double* lam, cudaStream_t st)
@@ -190,6 +258,9 @@ altob_status value_sumsq(const altob_tensor* t, double* acc, cudaStream_t st)
     template altob_status gram<FT>(const FT*, u64, int, double*, const double*, FT*, const FT*, double*,     \
                                    cudaStream_t);                                                            \
     template altob_status apply_w<FT>(FT*, u64, int, const double*, NormKind, double*, cudaStream_t);        \
+    template altob_status apply_gram<FT>(FT*, u64, int, const double*, NormKind, double*, double*, double*,  \
+                                         cudaStream_t);                                                      \
+    template altob_status normalize_cols<FT>(FT*, u64, int, const double*, cudaStream_t);                    \
     template altob_status colsum_abs<FT>(const FT*, u64, int, double*, cudaStream_t);                        \
     template altob_status div_cols<FT>(FT*, u64, int, const double*, cudaStream_t);                          \
     template altob_status mul_cols<FT>(FT*, u64, int, const double*, cudaStream_t);                          \

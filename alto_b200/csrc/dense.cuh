@@ -1,7 +1,8 @@
 // dense.cuh -- dense kernels of the CP-ALS / CP-APR updates.
 //
 // Reference operations replaced (IntelLabs/ALTO):
-//   update_gram (SYRK)          src/kruskal_model.cpp:11-24   -> k_gram (FP64 accumulate)
+//   update_gram (SYRK)          src/kruskal_model.cpp:11-24   -> k_gram (FP64 accumulate),
+//                                                               k_apply_gram (R <= 64, FP64 MMA)
 //   pseudo_inverse (POTRF/POTRS, GELSY fallback)
 //                               include/cpd.hpp:546-646       -> k_solve_setup + k_apply
 //   KruskalModelNorm            src/kruskal_model.cpp:224-341 -> k_apply (fused) + k_lambda
@@ -16,6 +17,7 @@ namespace altob {
 
 constexpr int DN_THREADS = 256;
 constexpr int SOLVE_MAX_RANK = 112;  // two R x R FP64 matrices in shared memory
+constexpr int APPLY_GRAM_MAX_RANK = 64;  // fused row update + Gram (up to eight 8-column MMA blocks)
 
 enum NormKind { NORM_NONE = 0, NORM_2 = 1, NORM_MAX = 2 };
 
@@ -30,6 +32,16 @@ altob_status solve_setup(const double* G, int nmode, int target, int R, double* 
 template <typename FT>
 altob_status apply_w(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, cudaStream_t st);
 altob_status lambda_from(const double* colacc, int R, NormKind nk, double* lam, cudaStream_t st);
+// Fused U <- U W with column statistics, G = U^T U and (inner given) the fit's
+// inner product, all before normalisation; lambda_finish then sets lambda,
+// G /= lambda lambda^T, inner /= lambda; normalize_cols divides U by lambda.
+template <typename FT>
+altob_status apply_gram(FT* U, u64 I, int R, const double* W, NormKind nk, double* colacc, double* G, double* inner,
+                        cudaStream_t st);
+altob_status lambda_finish(const double* colacc, int R, NormKind nk, double* lam, double* G, double* inner,
+                           cudaStream_t st);
+template <typename FT>
+altob_status normalize_cols(FT* U, u64 I, int R, const double* lam, cudaStream_t st);
 altob_status fit_from(const double* G, int nmode, int R, const double* lam, const double* inner, double normAT,
                       double* fit, cudaStream_t st);
 template <typename FT>

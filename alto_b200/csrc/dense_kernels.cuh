@@ -474,6 +474,309 @@ __global__ void __launch_bounds__(DN_THREADS) k_apply(FT* __restrict__ U, u64 I,
     apply_body<FT, LPR, CJ>(U, I, R, Wg, nk, colacc, blockIdx.x, gridDim.x);
 }
 
+// ------------------------------------------------ fused row update + Gram
+// One pass over the MTTKRP output M (held in U) for R <= 8*MB:
+//   Y = M W                      (FP64 tensor-core MMA, m8n8k4)
+//   U <- (FT) Y                  (in place)
+//   colacc: column 2-norm^2 / running max of the stored Y
+//   G' += Y^T Y                  (FP64 MMA over the rows of the warp's tile)
+//   inner'[r] += Y[:,r] . M[:,r] (when inner is given: the fit's inner product)
+// The caller then takes lambda from colacc, G = G' / (lambda lambda^T),
+// inner = inner' / lambda and divides U by lambda, which equals the
+// reference's apply -> normalise -> Gram order (cpd.hpp:102-163) up to the
+// rounding of the stored FT values.
+//
+// The product is formed transposed, Y^T = W^T M^T, so that the accumulator
+// fragment of an 8-row tile (lane (g, t) holds Y[r0 + 2t + i][8mb + g],
+// g = lane / 4, t = lane % 4) is directly the A and B operand of the Gram
+// MMA whose k index runs over the tile's rows (row r0 + 2k + i in MMA i):
+// no shuffles, no shared-memory transpose.  The k index of the row update is
+// permuted (input column t*KS + kk at k-step kk, lane slot t) so that each
+// lane's operand columns are contiguous in its row (vector loads).
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+constexpr int AG_THREADS = 128;
+constexpr int AG_WARPS = AG_THREADS / 32;
+
+// W^T fragments (later the block's Gram), column statistics and inner
+// partials per warp, and their block totals
+template <int MB>
+constexpr size_t apply_gram_smem()
+{
+    return (size_t)(64 * MB * MB + 2 * 8 * MB * (AG_WARPS + 1)) * sizeof(double);
+}
+
+// KS consecutive FT values of a row (columns c0.., zero beyond R).  Plain
+// loads, not the read-only path: the same warp overwrites the row later.
+template <typename FT, int KS>
+__device__ __forceinline__ void load_run(const FT* __restrict__ p, int c0, int R, bool full, bool row_ok, FT* v)
+{
+    constexpr int VB = (KS * (int)sizeof(FT)) % 16 == 0 ? 16 : (KS * (int)sizeof(FT)) % 8 == 0 ? 8 : 0;
+    if (VB && full && row_ok) {
+        constexpr int PER = VB ? VB / (int)sizeof(FT) : 1;
+#pragma unroll
+        for (int q = 0; q < KS / PER; ++q) {
+            if constexpr (VB == 16 && sizeof(FT) == 4) {
+                const float4 x = reinterpret_cast<const float4*>(p + c0)[q];
+                v[4 * q] = x.x, v[4 * q + 1] = x.y, v[4 * q + 2] = x.z, v[4 * q + 3] = x.w;
+            } else if constexpr (VB == 16) {
+                const double2 x = reinterpret_cast<const double2*>(p + c0)[q];
+                v[2 * q] = x.x, v[2 * q + 1] = x.y;
+            } else if constexpr (sizeof(FT) == 4) {
+                const float2 x = reinterpret_cast<const float2*>(p + c0)[q];
+                v[2 * q] = x.x, v[2 * q + 1] = x.y;
+            } else {
+                v[q] = p[c0 + q];
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < KS; ++k) v[k] = (row_ok && c0 + k < R) ? p[c0 + k] : FT(0);
+}
+
+template <typename FT, int MB>
+__device__ __forceinline__ void apply_gram_body(FT* __restrict__ U, u64 I, int R, const double* __restrict__ Wg,
+                                                int nk, double* __restrict__ colacc, double* __restrict__ G,
+                                                double* __restrict__ inner, int vec_ok, u64 bx, u64 nbx)
+{
+    constexpr int KS = 2 * MB;             // k-steps of the row update (4 input columns each)
+    constexpr int NB = MB * (MB + 1) / 2;  // Gram blocks a >= b
+    constexpr int RP = 8 * MB;             // rank padded to the MMA tile
+    // MB <= 4 keeps the column statistics in registers; larger blocks keep
+    // them per warp in shared memory to stay within 255 registers
+    constexpr bool SREG = MB <= 4;
+    extern __shared__ __align__(16) double ags[];
+    double* wf = ags;                 // MB*KS*32 W^T fragments in lane order; the Gram at the end
+    double* cw = wf + 64 * MB * MB;   // AG_WARPS x RP column statistics per warp
+    double* iw = cw + AG_WARPS * RP;  // AG_WARPS x RP inner partials per warp
+    double* cs = iw + AG_WARPS * RP;  // RP block column statistics
+    double* is = cs + RP;             // RP block inner partials
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const double sinit = nk == NORM_MAX ? 1.0 : 0.0;
+    for (int e = tid; e < MB * KS * 32; e += AG_THREADS) {
+        const int l = e & 31, kk = (e >> 5) % KS, mb = (e >> 5) / KS;
+        const int row = (l & 3) * KS + kk, col = 8 * mb + (l >> 2);
+        wf[e] = (row < R && col < R) ? Wg[row * R + col] : 0.0;
+    }
+    for (int e = tid; e < AG_WARPS * RP; e += AG_THREADS) {
+        cw[e] = sinit;
+        iw[e] = 0.0;
+    }
+    __syncthreads();
+    const bool full = R == RP && vec_ok;  // vector loads: whole rows, 16-byte aligned base
+    double gacc[NB][2], cst[SREG ? MB : 1], ipt[SREG ? MB : 1];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) gacc[q][0] = gacc[q][1] = 0.0;
+#pragma unroll
+    for (int mb = 0; mb < (SREG ? MB : 1); ++mb) {
+        cst[mb] = sinit;
+        ipt[mb] = 0.0;
+    }
+    const u64 step = nbx * (u64)AG_WARPS * 8;
+    for (u64 r0 = (bx * AG_WARPS + warp) * 8; r0 < I; r0 += step) {
+        FT bf[KS];
+        load_run<FT, KS>(U + (r0 + g) * R, t4 * KS, R, full, r0 + g < I, bf);
+        double y[MB][2];
+#pragma unroll
+        for (int mb = 0; mb < MB; ++mb) {
+            y[mb][0] = y[mb][1] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < KS; ++kk)
+                dmma884(y[mb][0], y[mb][1], wf[(mb * KS + kk) * 32 + lane], (double)bf[kk]);
+        }
+        // the inner product's M operand is read by the lane that overwrites
+        // it, just before the store (same thread, same address: ordered)
+        FT mv[MB][2];
+        if (inner) {
+#pragma unroll
+            for (int mb = 0; mb < MB; ++mb)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const u64 row = r0 + 2 * t4 + i;
+                    const int col = 8 * mb + g;
+                    mv[mb][i] = (row < I && col < R) ? U[row * R + col] : FT(0);
+                }
+        }
+#pragma unroll
+        for (int mb = 0; mb < MB; ++mb) {
+            double c = SREG ? cst[mb] : sinit, p = SREG ? ipt[mb] : 0.0;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const u64 row = r0 + 2 * t4 + i;
+                const int col = 8 * mb + g;
+                const FT yf = (FT)y[mb][i];
+                const double yd = (double)yf;
+                y[mb][i] = yd;  // rows past I and columns past R are exact zeros
+                if (row < I && col < R) U[row * R + col] = yf;
+                if (nk == NORM_2) c += yd * yd;
+                else if (nk == NORM_MAX) c = fmax(c, yd);
+                if (inner) p += yd * (double)mv[mb][i];
+            }
+            if constexpr (SREG) {
+                cst[mb] = c;
+                ipt[mb] = p;
+            } else {
+                // lanes g, t = 0..3 hold the same column: combine, one lane updates
+#pragma unroll
+                for (int o = 1; o <= 2; o <<= 1) {
+                    const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+                    c = nk == NORM_MAX ? fmax(c, c2) : c + c2;
+                    if (inner) p += __shfl_xor_sync(0xffffffffu, p, o);
+                }
+                if (t4 == 0) {
+                    double* cp = cw + warp * RP + 8 * mb + g;
+                    *cp = nk == NORM_MAX ? fmax(*cp, c) : *cp + c;
+                    if (inner) iw[warp * RP + 8 * mb + g] += p;
+                }
+            }
+        }
+        int q = 0;
+#pragma unroll
+        for (int a = 0; a < MB; ++a)
+#pragma unroll
+            for (int b = 0; b <= a; ++b, ++q) {
+                dmma884(gacc[q][0], gacc[q][1], y[a][0], y[b][0]);
+                dmma884(gacc[q][0], gacc[q][1], y[a][1], y[b][1]);
+            }
+    }
+    if constexpr (SREG) {
+#pragma unroll
+        for (int mb = 0; mb < MB; ++mb) {
+            double c = cst[mb], p = ipt[mb];
+#pragma unroll
+            for (int o = 1; o <= 2; o <<= 1) {
+                const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+                c = nk == NORM_MAX ? fmax(c, c2) : c + c2;
+                p += __shfl_xor_sync(0xffffffffu, p, o);
+            }
+            if (t4 == 0) {
+                cw[warp * RP + 8 * mb + g] = c;
+                iw[warp * RP + 8 * mb + g] = p;
+            }
+        }
+    }
+    __syncthreads();  // every warp is done with the W fragments: reuse them for the Gram
+    double* gs = wf;  // RP*RP
+    for (int e = tid; e < RP * RP; e += AG_THREADS) gs[e] = 0.0;
+    for (int r = tid; r < RP; r += AG_THREADS) {
+        double c = sinit, p = 0.0;
+        for (int w = 0; w < AG_WARPS; ++w) {
+            c = nk == NORM_MAX ? fmax(c, cw[w * RP + r]) : c + cw[w * RP + r];
+            p += iw[w * RP + r];
+        }
+        cs[r] = c;
+        is[r] = p;
+    }
+    __syncthreads();
+    {
+        int q = 0;
+#pragma unroll
+        for (int a = 0; a < MB; ++a)
+#pragma unroll
+            for (int b = 0; b <= a; ++b, ++q)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) atomicAdd(&gs[(8 * a + g) * RP + 8 * b + 2 * t4 + i], gacc[q][i]);
+    }
+    __syncthreads();
+    for (int e = tid; e < R * R; e += AG_THREADS) {
+        const int a = e / R, b = e - a * R;
+        if (a < b) continue;
+        const double v = gs[a * RP + b];  // block(a) >= block(b): computed
+        atomicAdd(&G[a * R + b], v);
+        if (a != b) atomicAdd(&G[b * R + a], v);
+    }
+    for (int r = tid; r < R; r += AG_THREADS) {
+        if (nk == NORM_2) atomicAdd(&colacc[r], cs[r]);
+        else if (nk == NORM_MAX) atomic_max_pos(&colacc[r], cs[r]);
+        if (inner) atomicAdd(&inner[r], is[r]);
+    }
+}
+
+template <typename FT, int MB>
+__global__ void __launch_bounds__(AG_THREADS) k_apply_gram(FT* __restrict__ U, u64 I, int R,
+                                                           const double* __restrict__ W, int nk,
+                                                           double* __restrict__ colacc, double* __restrict__ G,
+                                                           double* __restrict__ inner, int vec_ok)
+{
+    apply_gram_body<FT, MB>(U, I, R, W, nk, colacc, G, inner, vec_ok, blockIdx.x, gridDim.x);
+}
+
+// lambda from the column statistics, G = G' / (lambda lambda^T), inner /= lambda
+__device__ __forceinline__ void lambda_finish_body(const double* __restrict__ acc, int R, int nk,
+                                                   double* __restrict__ lam, double* __restrict__ G,
+                                                   double* __restrict__ inner)
+{
+    __shared__ double sl[SOLVE_MAX_RANK + 16];
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const double l = nk == NORM_2 ? sqrt(acc[r]) : acc[r];
+        sl[r] = l;
+        lam[r] = l;
+        if (inner) inner[r] /= l;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+        const int a = e / R, b = e - a * R;
+        G[e] = G[e] / sl[a] / sl[b];
+    }
+}
+
+static __global__ void k_lambda_finish(const double* acc, int R, int nk, double* lam, double* G, double* inner)
+{
+    lambda_finish_body(acc, R, nk, lam, G, inner);
+}
+
+// U[:, c] /= lambda[c] (FT storage, FP64 division as in the reference's
+// normalisation); VEC consecutive elements per thread (R % VEC == 0; 16-byte
+// vectors when VEC * sizeof(FT) == 16), the column index carried along the
+// grid-stride loop.
+template <typename FT, int VEC>
+__device__ __forceinline__ void div_cols_body(FT* __restrict__ U, u64 I, int R, const double* __restrict__ lam,
+                                              u64 bx, u64 nbx)
+{
+    extern __shared__ double dl_[];
+    for (int r = threadIdx.x; r < R; r += blockDim.x) dl_[r] = lam[r];
+    __syncthreads();
+    const u64 nv = I * (u64)R / VEC;
+    const u64 stride = nbx * blockDim.x;
+    u64 e = bx * blockDim.x + threadIdx.x;
+    if (e >= nv) return;
+    int col = (int)((e * VEC) % (u64)R);
+    const int cstep = (int)((stride * VEC) % (u64)R);
+    for (; e < nv; e += stride) {
+        union {
+            uint4 q;
+            FT f[VEC];
+        } v;
+        if constexpr (VEC * sizeof(FT) == 16) v.q = reinterpret_cast<const uint4*>(U)[e];
+        else
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) v.f[k] = U[e * VEC + k];
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) v.f[k] = (FT)((double)v.f[k] / dl_[col + k]);  // R % VEC == 0
+        if constexpr (VEC * sizeof(FT) == 16) reinterpret_cast<uint4*>(U)[e] = v.q;
+        else
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) U[e * VEC + k] = v.f[k];
+        col += cstep;
+        col = col >= R ? col - R : col;
+    }
+}
+
+template <typename FT, int VEC>
+__global__ void __launch_bounds__(DN_THREADS) k_div_cols(FT* __restrict__ U, u64 I, int R,
+                                                         const double* __restrict__ lam)
+{
+    div_cols_body<FT, VEC>(U, I, R, lam, blockIdx.x, gridDim.x);
+}
+
 // Rank classes of the row kernels: (lanes per row, columns per lane) and
 // Gram tiles per thread.
 inline int rank_class(int R) { return R <= 8 ? 0 : R <= 16 ? 1 : R <= 32 ? 2 : R <= 64 ? 3 : 4; }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <string>
 #include <vector>
@@ -251,6 +252,13 @@ altob_status tensor_scratch(altob_tensor* t, size_t bytes, void** out);
 altob_status tensor_hotbuf(altob_tensor* t, size_t bytes, void** out);
 
 int num_sms();
+
+// Integer setting from the environment (dflt when unset or empty).
+inline int env_int(const char* name, int dflt)
+{
+    const char* v = getenv(name);
+    return v && *v ? atoi(v) : dflt;
+}
 
 // Stable LSD radix sort of (key, payload) pairs on key bits [0, nbits).
 // Keys are kw u64 words (lo[], hi[]); payload is u32.  Ping-pong buffers

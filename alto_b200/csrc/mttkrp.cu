@@ -13,12 +13,6 @@
 
 namespace altob {
 
-static int env_int(const char* name, int dflt)
-{
-    const char* v = getenv(name);
-    return v && *v ? atoi(v) : dflt;
-}
-
 static int next_pow2(int x)
 {
     int p = 1;

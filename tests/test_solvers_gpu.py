@@ -190,3 +190,67 @@ def test_gpu_pseudo_inverse_fallback_matches_oracle(oracle, R):
     dU32 = torch.from_numpy(U.astype(np.float32)).cuda()
     assert ab.pseudo_inverse(torch.from_numpy(G).cuda(), 0, dU32)
     assert rel_fro(dU32.cpu().numpy(), want) < 1e-5
+
+
+@pytest.mark.parametrize("rank", [1, 5, 8, 13, 16, 27, 32, 33, 48, 64, 65])
+def test_gpu_cpd_fused_row_update_matches_oracle(oracle, rank, monkeypatch):
+    """Ranks up to 64 take the fused row-update + Gram pass (FP64 MMA), 65 the
+    separate passes; both against the oracle (FP64), and the fused FP64 result
+    against the separate passes (ALTOB_FUSED_APPLY=0)."""
+    torch = pytest.importorskip("torch")
+    dims, cidx, vals = synth.uniform_distinct((300, 200, 100), 60_000, seed=11)
+    at = ab.create_alto(_coo(dims, cidx, vals), 16, 0)
+    U, lam = oracle.random_init(dims, rank, 5)
+    ot = oracle.create(dims, cidx, vals, 16, 64)
+
+    def run(dtype):
+        dU = [torch.from_numpy(u.astype(dtype)).cuda() for u in U]
+        dl = torch.from_numpy(lam.astype(dtype)).cuda()
+        fits = ab.cpd_alto(at if dtype == np.float64 else at32, ab.KruskalModel([int(d) for d in dims], rank, dU, dl),
+                           6, 1e-30)
+        return fits, [u.cpu().numpy() for u in dU], dl.cpu().numpy()
+
+    at32 = ab.create_alto(_coo(dims, cidx, vals), 16, 0, val_dtype="f32")
+    oU = [u.copy() for u in U]
+    ofits = ot.cpd_als(oU, lam.copy(), rank, 6, 1e-30)
+    fits, gU, glam = run(np.float64)
+    np.testing.assert_allclose(fits, ofits, rtol=1e-9)
+    for n in range(3):
+        assert rel_fro(gU[n], oU[n]) < 1e-8, n
+    monkeypatch.setenv("ALTOB_FUSED_APPLY", "0")
+    fits0, gU0, glam0 = run(np.float64)
+    monkeypatch.delenv("ALTOB_FUSED_APPLY")
+    assert np.max(np.abs(fits - fits0)) < 1e-12
+    for n in range(3):
+        assert rel_fro(gU[n], gU0[n]) < 1e-11, n
+    np.testing.assert_allclose(glam, glam0, rtol=1e-11)
+    fits32, _, _ = run(np.float32)
+    assert np.max(np.abs(fits32 - ofits)) < 1e-4
+
+
+@pytest.mark.parametrize("rank", [16, 24, 32, 64])
+def test_gpu_cpd_fused_row_update_unaligned_factors(rank):
+    """Factor matrices that start 4 bytes past a 16-byte boundary take the
+    scalar loads of the fused pass (and of the MTTKRP); same fits as aligned
+    factors."""
+    torch = pytest.importorskip("torch")
+    dims, cidx, vals = synth.uniform_distinct((400, 150, 90), 50_000, seed=12)
+    at = ab.create_alto(_coo(dims, cidx, vals), 16, 0, val_dtype="f32")
+    M = ab.random_init_factors(dims, rank, 8, dtype=np.float32)
+
+    def run(offset):
+        dU = []
+        for u in M.U:
+            buf = torch.zeros(u.size + offset, dtype=torch.float32, device="cuda")
+            v = buf[offset:].view(u.shape)
+            v.copy_(torch.from_numpy(u))
+            dU.append(v)
+        dl = torch.from_numpy(M.lam.copy()).cuda()
+        fits = ab.cpd_alto(at, ab.KruskalModel([int(d) for d in dims], rank, dU, dl), 5, 1e-30)
+        return fits, [u.cpu().numpy() for u in dU]
+
+    fa, ua = run(0)
+    fu, uu = run(1)
+    assert np.max(np.abs(fa - fu)) < 1e-6
+    for n in range(3):
+        assert rel_fro(uu[n], ua[n]) < 1e-4, n
