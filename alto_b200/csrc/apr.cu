@@ -143,18 +143,25 @@ static altob_status loglik_impl(altob_tensor* t, FT** U, double* lam, double* co
     return ALTOB_OK;
 }
 
-// Precomputed Khatri-Rao rows (the reference's PRE build) when a mode runs
-// more than one inner iteration and the nnz x R buffer is small next to free
-// memory; ALTOB_APR_PHI=pre|otf forces either path.
-static bool apr_use_pre(const altob_tensor* t, int R, size_t fsz, int max_inner)
+// How Phi is formed: precomputed Khatri-Rao rows (the reference's PRE build)
+// when a mode runs more than one inner iteration, in the row-ordered stream
+// (PHI_ROWS: rows, values and stream positions kept per mode) when that fits
+// in a quarter of free memory, else in ALTO order (PHI_PRE, the tiled
+// kernel), else on the fly (PHI_OTF).  ALTOB_APR_PHI=rows|pre|otf forces one.
+enum AprPhi { PHI_OTF = 0, PHI_PRE = 1, PHI_ROWS = 2 };
+
+static AprPhi apr_phi_kind(const altob_tensor* t, int R, size_t fsz, int max_inner)
 {
     const char* v = getenv("ALTOB_APR_PHI");
-    if (v && !strcmp(v, "otf")) return false;
-    if (v && !strcmp(v, "pre")) return true;
-    if (max_inner < 2) return false;
+    if (v && !strcmp(v, "otf")) return PHI_OTF;
+    if (v && !strcmp(v, "pre")) return PHI_PRE;
+    if (v && !strcmp(v, "rows")) return PHI_ROWS;
+    if (max_inner < 2) return PHI_OTF;
     size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
-    return (double)t->nnz * R * fsz <= 0.25 * (double)fr;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return PHI_OTF;
+    const double nnz = (double)t->nnz;
+    if (nnz * ((double)R * fsz + t->nmode * (8.0 + fsz) + 24.0) <= 0.25 * (double)fr) return PHI_ROWS;
+    return nnz * R * fsz <= 0.25 * (double)fr ? PHI_PRE : PHI_OTF;
 }
 
 template <typename FT>
@@ -206,11 +213,35 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
     std::vector<double> kkt_iter(max_iters + 1, 0.0), kmode(N, 0.0);
     std::vector<int> ninner(max_iters + 1, 0);
     void* pi = nullptr;  // nnz x R precomputed rows
-    if (t->nnz && apr_use_pre(t, R, sizeof(FT), max_inner)) ALTOB_TRY(dmalloc(&pi, t->nnz * (size_t)R * sizeof(FT)));
+    u32 *rows = nullptr, *inv = nullptr;  // row-ordered stream: N x nnz each
+    FT* svals = nullptr;
     struct PiFree {
-        void* p;
-        ~PiFree() { dfree(p); }
-    } pi_free{pi};
+        void *p, *r, *i, *v;
+        ~PiFree()
+        {
+            dfree(p);
+            dfree(r);
+            dfree(i);
+            dfree(v);
+        }
+    } pi_free{nullptr, nullptr, nullptr, nullptr};
+    const u64 nnz = t->nnz;
+    const AprPhi kind = nnz ? apr_phi_kind(t, R, sizeof(FT), max_inner) : PHI_OTF;
+    if (kind == PHI_ROWS) {
+        ALTOB_TRY(dmalloc_t(&rows, (size_t)N * nnz));
+        pi_free.r = rows;
+        ALTOB_TRY(dmalloc_t(&inv, (size_t)N * nnz));
+        pi_free.i = inv;
+        ALTOB_TRY(dmalloc_t(&svals, (size_t)N * nnz));
+        pi_free.v = svals;
+        for (int n = 0; n < N; ++n)
+            ALTOB_TRY(mode_order_device(t, n, ft, rows + (size_t)n * nnz, svals + (size_t)n * nnz,
+                                        inv + (size_t)n * nnz, st));
+    }
+    if (kind != PHI_OTF) {
+        ALTOB_TRY(dmalloc(&pi, nnz * (size_t)R * sizeof(FT)));
+        pi_free.p = pi;
+    }
     int iter;
     for (iter = 0; iter < max_iters; ++iter) {
         bool converged = false;
@@ -224,10 +255,14 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
             }
             ALTOB_TRY(mul_cols<FT>(B, t->dims[n], R, s.lam, st));  // RedistributeLambda
             ALTOB_TRY(vec_fill(s.lam, R, 1.0, st));
-            if (pi) ALTOB_TRY(pi_device(t, n, ft, (void* const*)U, (u64)R, pi, st));
+            const u32* inv_n = rows ? inv + (size_t)n * nnz : nullptr;
+            if (pi) ALTOB_TRY(pi_device(t, n, ft, (void* const*)U, (u64)R, pi, st, inv_n));
             for (int inner = 0; inner < max_inner; ++inner) {
                 ninner[iter]++;
-                if (pi) ALTOB_TRY(phi_pre_device(t, n, ft, pi, B, (u64)R, eps_div_zero, Phi[n], st));
+                if (rows)
+                    ALTOB_TRY(phi_rows_device(t, n, ft, pi, rows + (size_t)n * nnz, svals + (size_t)n * nnz, B,
+                                              (u64)R, eps_div_zero, Phi[n], st));
+                else if (pi) ALTOB_TRY(phi_pre_device(t, n, ft, pi, B, (u64)R, eps_div_zero, Phi[n], st));
                 else ALTOB_TRY(phi_device(t, n, ft, (void* const*)U, (u64)R, eps_div_zero, Phi[n], st));
                 if (dobench) {
                     // no early exit: the violation of the last round is what the reference reports

@@ -235,6 +235,7 @@ struct PiArgs {
     int nmode, target, R;
     const FT* U[ALTOB_MAX_MODES];
     FT* Pi;
+    const u32* inv;  // row of nonzero i in Pi (row-ordered stream), or nullptr: row i
 };
 
 template <typename FT, int NM, int VEC>
@@ -262,7 +263,8 @@ __global__ void __launch_bounds__(256) k_pi(PiArgs<FT> a)
             vmul<FT, VEC>(x, y);
         }
         typedef typename VecT<FT, VEC>::T V;
-        *reinterpret_cast<V*>(a.Pi + i * a.R + c) = *reinterpret_cast<const V*>(x);
+        const u64 dst = a.inv ? (u64)a.inv[i] : i;
+        *reinterpret_cast<V*>(a.Pi + dst * a.R + c) = *reinterpret_cast<const V*>(x);
     }
 }
 
@@ -275,7 +277,8 @@ static void launch_pi_nm(const PiArgs<FT>& a, int vec, int grid, cudaStream_t st
 }
 
 template <typename FT>
-static altob_status pi_rows(altob_tensor* t, int mode, void* const* dU, u64 R, void* dpi, cudaStream_t st)
+static altob_status pi_rows(altob_tensor* t, int mode, void* const* dU, u64 R, void* dpi, const u32* inv,
+                           cudaStream_t st)
 {
     PiArgs<FT> a;
     memset(&a, 0, sizeof(a));
@@ -291,6 +294,7 @@ static altob_status pi_rows(altob_tensor* t, int mode, void* const* dU, u64 R, v
         aligned = aligned && ptr_aligned16(dU[m]);
     }
     a.Pi = (FT*)dpi;
+    a.inv = inv;
     constexpr int V = 16 / sizeof(FT);
     const int vec = (aligned && R % V == 0) ? V : 1;
     const u64 work = t->nnz * (R / vec);
@@ -305,12 +309,231 @@ static altob_status pi_rows(altob_tensor* t, int mode, void* const* dU, u64 R, v
     return ALTOB_OK;
 }
 
-altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, void* dpi, cudaStream_t st)
+altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, void* dpi, cudaStream_t st,
+                       const u32* inv)
 {
     if (!t || !dU || !dpi) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
     if (t->nnz == 0) return ALTOB_OK;
-    return ft == ALTOB_F64 ? pi_rows<double>(t, mode, dU, R, dpi, st) : pi_rows<float>(t, mode, dU, R, dpi, st);
+    return ft == ALTOB_F64 ? pi_rows<double>(t, mode, dU, R, dpi, inv, st)
+                           : pi_rows<float>(t, mode, dU, R, dpi, inv, st);
+}
+
+// ------------------------------------- CP-APR Phi over a row-ordered stream
+// For target mode n the nonzeros are put once in the order of their mode-n
+// index (a stable LSD radix sort of (index, position) pairs): rows[k] is the
+// target row of stream position k, vals[k] its value and inv[i] the stream
+// position of nonzero i.  k_pi then writes the Khatri-Rao row of nonzero i
+// to stream row inv[i], so every inner iteration reads keys-free, fully
+// sequential rows: Phi[r] = sum over the run of row r of
+// (v / max(B[r] . pi, eps)) pi, the products and the dot product formed as in
+// the tiled Phi (apr.hpp:383-848 computes the same sums per row).  A warp
+// takes PR_CHUNK consecutive stream positions; each lane group keeps the
+// running sum of its current row in registers and adds it to Phi with one
+// vector atomic when the row changes (rows change rarely: the runs of a
+// mode are nnz / dims long on average).
+
+constexpr u64 PR_CHUNK = 2048;
+constexpr int PR_THREADS = 256;
+
+__global__ void k_mode_idx(KeySrc key, Fields fld, int mode, u64 n, u64* __restrict__ idx, u32* __restrict__ iota)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 lo = key.klo[i], hi = key_hi(key, i);
+        idx[i] = field(lo, hi, fld.pos[mode], fld.mask[mode]);
+        iota[i] = (u32)i;
+    }
+}
+
+template <typename FT, typename VT>
+__global__ void k_row_meta(const u64* __restrict__ sidx, const u32* __restrict__ perm, const VT* __restrict__ vals,
+                           u64 n, u32* __restrict__ rows, FT* __restrict__ svals, u32* __restrict__ inv)
+{
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x) {
+        const u32 p = perm[k];
+        rows[k] = (u32)sidx[k];
+        svals[k] = (FT)vals[p];
+        inv[p] = (u32)k;
+    }
+}
+
+template <typename FT, int VEC, int LPN, int CH>
+__global__ void __launch_bounds__(PR_THREADS) k_phi_rows(const FT* __restrict__ Pi, const u32* __restrict__ rows,
+                                                         const FT* __restrict__ vals, const FT* __restrict__ B,
+                                                         FT* __restrict__ Phi, u64 nnz, int R, FT eps)
+{
+    constexpr int G = 32 / LPN;  // nonzeros per warp step
+    constexpr int UN = 2;        // steps whose loads are issued together
+    const int lane = threadIdx.x & 31, grp = lane / LPN, sub = lane % LPN;
+    const unsigned gmask = LPN == 32 ? 0xffffffffu : (((1u << LPN) - 1u) << (grp * LPN));
+    const u64 nchunks = (nnz + PR_CHUNK - 1) / PR_CHUNK;
+    const u64 nw = ((u64)gridDim.x * blockDim.x) >> 5;
+    for (u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nw) {
+        const u64 k1 = min(nnz, (c + 1) * PR_CHUNK);
+        u32 cur = 0xffffffffu;
+        FT acc[CH][VEC];
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) acc[ch][e] = FT(0);
+        for (u64 k = c * PR_CHUNK + grp; k < k1; k += (u64)G * UN) {
+            u32 rw[UN];
+            FT v[UN], x[UN][CH][VEC];
+#pragma unroll
+            for (int u = 0; u < UN; ++u) {
+                const u64 ku = k + (u64)u * G;
+                const bool ok = ku < k1;
+                rw[u] = ok ? __ldcs(rows + ku) : 0xffffffffu;
+                v[u] = ok ? __ldcs(vals + ku) : FT(0);
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch) {
+                    const int r0 = ch * LPN * VEC + sub * VEC;
+                    if (ok && r0 < R) vload_stream<FT, VEC>(Pi + ku * R + r0, x[u][ch]);
+                    else
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) x[u][ch][e] = FT(0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UN; ++u) {
+                if (rw[u] == 0xffffffffu) break;  // past the chunk (uniform in the group)
+                if (rw[u] != cur) {
+                    if (cur != 0xffffffffu)
+#pragma unroll
+                        for (int ch = 0; ch < CH; ++ch) {
+                            const int r0 = ch * LPN * VEC + sub * VEC;
+                            if (r0 < R) gred<FT, VEC>(Phi + (size_t)cur * R + r0, acc[ch]);
+                        }
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) acc[ch][e] = FT(0);
+                    cur = rw[u];
+                }
+                const FT* brow = B + (size_t)rw[u] * R;
+                FT dot = FT(0);
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch) {
+                    const int r0 = ch * LPN * VEC + sub * VEC;
+                    if (r0 < R) {
+                        FT b[VEC];
+                        vload<FT, VEC>(brow + r0, b);
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) dot += b[e] * x[u][ch][e];
+                    }
+                }
+#pragma unroll
+                for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(gmask, dot, o, LPN);
+                const FT sc = v[u] / (dot > eps ? dot : eps);
+#pragma unroll
+                for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) acc[ch][e] += x[u][ch][e] * sc;
+            }
+        }
+        if (cur != 0xffffffffu)
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) {
+                const int r0 = ch * LPN * VEC + sub * VEC;
+                if (r0 < R) gred<FT, VEC>(Phi + (size_t)cur * R + r0, acc[ch]);
+            }
+    }
+}
+
+template <typename FT, typename VT>
+static altob_status mode_order_vt(altob_tensor* t, int mode, u32* rows, FT* svals, u32* inv, cudaStream_t st)
+{
+    const u64 n = t->nnz;
+    u64 *mk = nullptr, *mk2 = nullptr;
+    u32 *p = nullptr, *p2 = nullptr;
+    altob_status s = dmalloc_t(&mk, n);
+    if (s == ALTOB_OK) s = dmalloc_t(&mk2, n);
+    if (s == ALTOB_OK) s = dmalloc_t(&p, n);
+    if (s == ALTOB_OK) s = dmalloc_t(&p2, n);
+    int bits = 0;
+    while (bits < 32 && (1ull << bits) < t->dims[mode]) ++bits;
+    const int grid = (int)std::max<u64>(1, std::min<u64>((n + 255) / 256, (u64)num_sms() * 8));
+    bool alt = false;
+    if (s == ALTOB_OK) {
+        k_mode_idx<<<grid, 256, 0, st>>>(key_src(t), t->fld, mode, n, mk, p);
+        s = cudaGetLastError() == cudaSuccess ? ALTOB_OK : fail(ALTOB_ERR_CUDA, "mode index launch failed");
+    }
+    if (s == ALTOB_OK) s = radix_sort_pairs(mk, nullptr, p, mk2, nullptr, p2, n, 1, bits, st, &alt);
+    if (s == ALTOB_OK) {
+        k_row_meta<FT, VT><<<grid, 256, 0, st>>>(alt ? mk2 : mk, alt ? p2 : p, (const VT*)t->d_vals, n, rows, svals,
+                                                 inv);
+        s = cudaGetLastError() == cudaSuccess ? ALTOB_OK : fail(ALTOB_ERR_CUDA, "row order launch failed");
+    }
+    dfree(mk);
+    dfree(mk2);
+    dfree(p);
+    dfree(p2);
+    return s;
+}
+
+altob_status mode_order_device(altob_tensor* t, int mode, altob_dtype ft, u32* rows, void* svals, u32* inv,
+                               cudaStream_t st)
+{
+    if (!t || !rows || !svals || !inv) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    if (t->nnz == 0) return ALTOB_OK;
+    const bool f64 = ft == ALTOB_F64;
+    if (t->vdt == ALTOB_U32)
+        return f64 ? mode_order_vt<double, u32>(t, mode, rows, (double*)svals, inv, st)
+                   : mode_order_vt<float, u32>(t, mode, rows, (float*)svals, inv, st);
+    if ((t->vdt == ALTOB_F64) != f64)
+        return fail(ALTOB_ERR_UNSUPPORTED, "stored value dtype does not match the compute dtype");
+    return f64 ? mode_order_vt<double, double>(t, mode, rows, (double*)svals, inv, st)
+               : mode_order_vt<float, float>(t, mode, rows, (float*)svals, inv, st);
+}
+
+template <typename FT, int VEC>
+static void launch_phi_rows(int lpn, int ch, int grid, const FT* pi, const u32* rows, const FT* vals, const FT* B,
+                            FT* phi, u64 nnz, int R, FT eps, cudaStream_t st)
+{
+#define PRK(L, C) k_phi_rows<FT, VEC, L, C><<<grid, PR_THREADS, 0, st>>>(pi, rows, vals, B, phi, nnz, R, eps)
+    if (ch == 4) PRK(32, 4);
+    else if (ch == 2) PRK(32, 2);
+    else if (lpn == 32) PRK(32, 1);
+    else if (lpn == 16) PRK(16, 1);
+    else if (lpn == 8) PRK(8, 1);
+    else if (lpn == 4) PRK(4, 1);
+    else if (lpn == 2) PRK(2, 1);
+    else PRK(1, 1);
+#undef PRK
+}
+
+altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
+                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st)
+{
+    if (!t || !dpi || !rows || !svals || !dB || !dphi) return fail(ALTOB_ERR_ARG, "NULL argument");
+    if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
+    if (R == 0 || R > 128) return fail(ALTOB_ERR_UNSUPPORTED, "rank must be 1..128");
+    const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_CUDA(cudaMemsetAsync(dphi, 0, t->dims[mode] * R * fsz, st));
+    if (t->nnz == 0) return ALTOB_OK;
+    const int V = (int)(16 / fsz);
+    const bool vec = R % V == 0 && ptr_aligned16(dpi) && ptr_aligned16(dB) && ptr_aligned16(dphi);
+    const int ve = vec ? V : 1;
+    int lpn = 1;
+    while (lpn < 32 && (u64)lpn * ve < R) lpn <<= 1;
+    const int ch = (int)((R + (u64)lpn * ve - 1) / ((u64)lpn * ve));  // 1, 2 or 4 (only with 32 lanes)
+    const u64 nchunks = (t->nnz + PR_CHUNK - 1) / PR_CHUNK;
+    const int grid = (int)std::max<u64>(1, std::min<u64>((nchunks + 7) / 8, (u64)num_sms() * 8));
+    const u64 nnz = t->nnz;
+    if (ft == ALTOB_F64) {
+        if (vec) launch_phi_rows<double, 2>(lpn, ch, grid, (const double*)dpi, rows, (const double*)svals,
+                                            (const double*)dB, (double*)dphi, nnz, (int)R, eps, st);
+        else launch_phi_rows<double, 1>(lpn, ch, grid, (const double*)dpi, rows, (const double*)svals,
+                                        (const double*)dB, (double*)dphi, nnz, (int)R, eps, st);
+    } else {
+        if (vec) launch_phi_rows<float, 4>(lpn, ch, grid, (const float*)dpi, rows, (const float*)svals,
+                                           (const float*)dB, (float*)dphi, nnz, (int)R, (float)eps, st);
+        else launch_phi_rows<float, 1>(lpn, ch, grid, (const float*)dpi, rows, (const float*)svals,
+                                       (const float*)dB, (float*)dphi, nnz, (int)R, (float)eps, st);
+    }
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
 }
 
 // Phi of mode `mode` from precomputed rows `dpi` and the current factor B.

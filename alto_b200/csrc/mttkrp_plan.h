@@ -20,9 +20,17 @@ altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* 
                         void* dphi, cudaStream_t st);
 // Khatri-Rao rows of every nonzero for `mode` (nnz x R, ALTO order) and Phi
 // computed from them (CP-APR with precomputed rows).
+// inv given: row i goes to stream row inv[i] (the row-ordered stream below).
 altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, void* dpi,
-                       cudaStream_t st);
+                       cudaStream_t st, const u32* inv = nullptr);
 altob_status phi_pre_device(altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const void* dB, u64 R,
                             double eps, void* dphi, cudaStream_t st);
+// Row-ordered stream of `mode` (CP-APR): rows[k], vals[k] (compute dtype)
+// of the k-th nonzero in mode-index order, inv[i] = stream position of
+// nonzero i; and Phi computed from it and the stream-ordered Khatri-Rao rows.
+altob_status mode_order_device(altob_tensor* t, int mode, altob_dtype ft, u32* rows, void* svals, u32* inv,
+                               cudaStream_t st);
+altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
+                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st);
 
 }  // namespace altob

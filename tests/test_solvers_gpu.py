@@ -73,11 +73,11 @@ def test_gpu_cpd_device_model_matches_oracle(oracle):
         assert rel_fro(dU[n].cpu().numpy(), U[n]) < 1e-8
 
 
-@pytest.mark.parametrize("phi", ["pre", "otf"])
+@pytest.mark.parametrize("phi", ["rows", "pre", "otf"])
 @pytest.mark.parametrize("name", ["apr_bench", "apr_eps"])
 def test_gpu_cp_apr_fp64_matches_reference_fixture(name, phi, monkeypatch):
-    """Both Phi paths (precomputed Khatri-Rao rows, on the fly) against the
-    reference's own output."""
+    """Every Phi path (precomputed Khatri-Rao rows in the row-ordered stream
+    or in ALTO order, on the fly) against the reference's own output."""
     monkeypatch.setenv("ALTOB_APR_PHI", phi)
     g = load_golden(name)
     rank = int(g["rank"])
@@ -93,7 +93,7 @@ def test_gpu_cp_apr_fp64_matches_reference_fixture(name, phi, monkeypatch):
         assert rel_fro(M.U[n], g[f"U{n}"]) < 1e-8
 
 
-@pytest.mark.parametrize("phi", ["pre", "otf"])
+@pytest.mark.parametrize("phi", ["rows", "pre", "otf"])
 def test_gpu_cp_apr_early_exit_and_fp32(oracle, phi, monkeypatch):
     monkeypatch.setenv("ALTOB_APR_PHI", phi)
     dims, cidx, vals = synth.poisson_kruskal((200, 150, 100, 20), 6, 200_000, seed=6)
@@ -117,6 +117,25 @@ def test_gpu_cp_apr_early_exit_and_fp32(oracle, phi, monkeypatch):
     got = ab.cp_apr_alto(at, M32, 6, 5, epsilon=0.0, dobench=True)
     assert abs(got["loglik"] - want["loglik"]) <= 1e-4 * abs(want["loglik"])
     assert abs(got["fit"] - want["fit"]) <= 1e-4
+
+
+@pytest.mark.parametrize("rank", [3, 16, 40, 100])
+def test_gpu_cp_apr_row_stream_matches_on_the_fly(rank, monkeypatch):
+    """The row-ordered Phi for every lane layout (ranks below, at and above
+    one vector per lane group; 2 and 4 chunks per lane) against the
+    on-the-fly Phi, FP64 and FP32, fixed inner counts."""
+    dims, cidx, vals = synth.poisson_kruskal((300, 120, 80, 15), 5, 150_000, seed=21)
+    at = ab.create_alto(_coo(dims, cidx, vals), 8, 0, val_dtype="u32")
+    for dtype, tol in ((np.float64, 1e-10), (np.float32, 1e-4)):
+        res = {}
+        for phi in ("rows", "otf"):
+            monkeypatch.setenv("ALTOB_APR_PHI", phi)
+            M = ab.random_init_factors(dims, rank, 3, dtype=dtype)
+            res[phi] = (ab.cp_apr_alto(at, M, 4, 5, epsilon=0.0, dobench=True), M)
+        (ra, Ma), (rb, Mb) = res["rows"], res["otf"]
+        assert abs(ra["loglik"] - rb["loglik"]) <= tol * abs(rb["loglik"])
+        for n in range(4):
+            assert rel_fro(Ma.U[n], Mb.U[n]) < (1e-9 if dtype == np.float64 else 1e-3), n
 
 
 def test_gpu_phi_and_loglik_match_oracle(oracle):
