@@ -333,7 +333,7 @@ altob_status pi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* d
 // vector atomic when the row changes (rows change rarely: the runs of a
 // mode are nnz / dims long on average).
 
-constexpr u64 PR_CHUNK = 2048;
+constexpr u64 PR_CHUNK = 512;
 constexpr int PR_THREADS = 256;
 
 __global__ void k_mode_idx(KeySrc key, Fields fld, int mode, u64 n, u64* __restrict__ idx, u32* __restrict__ iota)
@@ -357,13 +357,94 @@ __global__ void k_row_meta(const u64* __restrict__ sidx, const u32* __restrict__
     }
 }
 
+// UN nonzeros of a lane group (stream positions k, k + G, ...; rw = ~0 past k1)
+template <typename FT, int VEC, int LPN, int CH, int UN>
+struct RowStep {
+    u32 rw[UN];
+    FT v[UN], x[UN][CH][VEC];
+    __device__ __forceinline__ void load(const FT* __restrict__ Pi, const u32* __restrict__ rows,
+                                         const FT* __restrict__ vals, u64 k, u64 k1, int R, int sub)
+    {
+        constexpr int G = 32 / LPN;
+#pragma unroll
+        for (int u = 0; u < UN; ++u) {
+            const u64 ku = k + (u64)u * G;
+            const bool ok = ku < k1;
+            rw[u] = ok ? __ldcs(rows + ku) : 0xffffffffu;
+            v[u] = ok ? __ldcs(vals + ku) : FT(0);
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) {
+                const int r0 = ch * LPN * VEC + sub * VEC;
+                if (ok && r0 < R) vload_stream<FT, VEC>(Pi + ku * R + r0, x[u][ch]);
+                else
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) x[u][ch][e] = FT(0);
+            }
+        }
+    }
+};
+
+// Adds the step's nonzeros to the lane group's run; a row change flushes the
+// run with one vector atomic per lane and reloads the cached B row.
+template <typename FT, int VEC, int LPN, int CH, int UN>
+__device__ __forceinline__ void row_step(const RowStep<FT, VEC, LPN, CH, UN>& s, const FT* __restrict__ B,
+                                         FT* __restrict__ Phi, int R, int sub, unsigned gmask, FT eps, u32& cur,
+                                         FT (*acc)[VEC], FT (*bc)[VEC])
+{
+#pragma unroll
+    for (int u = 0; u < UN; ++u) {
+        if (s.rw[u] == 0xffffffffu) break;  // past the chunk (uniform in the group)
+        if (s.rw[u] != cur) {
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) {
+                const int r0 = ch * LPN * VEC + sub * VEC;
+                if (r0 < R) {
+                    if (cur != 0xffffffffu) gred<FT, VEC>(Phi + (size_t)cur * R + r0, acc[ch]);
+                    vload<FT, VEC>(B + (size_t)s.rw[u] * R + r0, bc[ch]);
+                }
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) acc[ch][e] = FT(0);
+            }
+            cur = s.rw[u];
+        }
+        FT dot = FT(0);
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+            const int r0 = ch * LPN * VEC + sub * VEC;
+            if (r0 < R)
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) dot += bc[ch][e] * s.x[u][ch][e];
+        }
+#pragma unroll
+        for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(gmask, dot, o, LPN);
+        const FT sc = s.v[u] / (dot > eps ? dot : eps);
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch)
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) acc[ch][e] += s.x[u][ch][e] * sc;
+    }
+}
+
+// Resident blocks per SM the register budget is set for: while a lane holds
+// at most 16 bytes of a stream row, four (64 registers) in FP32 and three in
+// FP64; else two.
+template <typename FT, int VEC, int CH>
+constexpr int pr_min_blocks()
+{
+    return CH * VEC * (int)sizeof(FT) <= 16 ? (sizeof(FT) == 4 ? 4 : 3) : 2;
+}
+
+// Two register buffers of UN steps: the loads of the next buffer are issued
+// before the current one is reduced, so a warp keeps 2 x UN x G stream rows
+// in flight.
 template <typename FT, int VEC, int LPN, int CH>
-__global__ void __launch_bounds__(PR_THREADS) k_phi_rows(const FT* __restrict__ Pi, const u32* __restrict__ rows,
+__global__ void __launch_bounds__(PR_THREADS, pr_min_blocks<FT, VEC, CH>()) k_phi_rows(const FT* __restrict__ Pi, const u32* __restrict__ rows,
                                                          const FT* __restrict__ vals, const FT* __restrict__ B,
                                                          FT* __restrict__ Phi, u64 nnz, int R, FT eps)
 {
     constexpr int G = 32 / LPN;  // nonzeros per warp step
-    constexpr int UN = 2;        // steps whose loads are issued together
+    constexpr int UN = 2;
+    constexpr u64 S = (u64)G * UN;
     const int lane = threadIdx.x & 31, grp = lane / LPN, sub = lane % LPN;
     const unsigned gmask = LPN == 32 ? 0xffffffffu : (((1u << LPN) - 1u) << (grp * LPN));
     const u64 nchunks = (nnz + PR_CHUNK - 1) / PR_CHUNK;
@@ -371,65 +452,22 @@ __global__ void __launch_bounds__(PR_THREADS) k_phi_rows(const FT* __restrict__ 
     for (u64 c = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nw) {
         const u64 k1 = min(nnz, (c + 1) * PR_CHUNK);
         u32 cur = 0xffffffffu;
-        FT acc[CH][VEC];
+        FT acc[CH][VEC], bc[CH][VEC];
 #pragma unroll
         for (int ch = 0; ch < CH; ++ch)
 #pragma unroll
-            for (int e = 0; e < VEC; ++e) acc[ch][e] = FT(0);
-        for (u64 k = c * PR_CHUNK + grp; k < k1; k += (u64)G * UN) {
-            u32 rw[UN];
-            FT v[UN], x[UN][CH][VEC];
-#pragma unroll
-            for (int u = 0; u < UN; ++u) {
-                const u64 ku = k + (u64)u * G;
-                const bool ok = ku < k1;
-                rw[u] = ok ? __ldcs(rows + ku) : 0xffffffffu;
-                v[u] = ok ? __ldcs(vals + ku) : FT(0);
-#pragma unroll
-                for (int ch = 0; ch < CH; ++ch) {
-                    const int r0 = ch * LPN * VEC + sub * VEC;
-                    if (ok && r0 < R) vload_stream<FT, VEC>(Pi + ku * R + r0, x[u][ch]);
-                    else
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) x[u][ch][e] = FT(0);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < UN; ++u) {
-                if (rw[u] == 0xffffffffu) break;  // past the chunk (uniform in the group)
-                if (rw[u] != cur) {
-                    if (cur != 0xffffffffu)
-#pragma unroll
-                        for (int ch = 0; ch < CH; ++ch) {
-                            const int r0 = ch * LPN * VEC + sub * VEC;
-                            if (r0 < R) gred<FT, VEC>(Phi + (size_t)cur * R + r0, acc[ch]);
-                        }
-#pragma unroll
-                    for (int ch = 0; ch < CH; ++ch)
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) acc[ch][e] = FT(0);
-                    cur = rw[u];
-                }
-                const FT* brow = B + (size_t)rw[u] * R;
-                FT dot = FT(0);
-#pragma unroll
-                for (int ch = 0; ch < CH; ++ch) {
-                    const int r0 = ch * LPN * VEC + sub * VEC;
-                    if (r0 < R) {
-                        FT b[VEC];
-                        vload<FT, VEC>(brow + r0, b);
-#pragma unroll
-                        for (int e = 0; e < VEC; ++e) dot += b[e] * x[u][ch][e];
-                    }
-                }
-#pragma unroll
-                for (int o = LPN / 2; o > 0; o >>= 1) dot += __shfl_xor_sync(gmask, dot, o, LPN);
-                const FT sc = v[u] / (dot > eps ? dot : eps);
-#pragma unroll
-                for (int ch = 0; ch < CH; ++ch)
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) acc[ch][e] += x[u][ch][e] * sc;
-            }
+            for (int e = 0; e < VEC; ++e) acc[ch][e] = bc[ch][e] = FT(0);
+        RowStep<FT, VEC, LPN, CH, UN> a, b;
+        u64 k = c * PR_CHUNK + grp;
+        a.load(Pi, rows, vals, k, k1, R, sub);
+        while (k < k1) {
+            b.load(Pi, rows, vals, k + S, k1, R, sub);
+            row_step(a, B, Phi, R, sub, gmask, eps, cur, acc, bc);
+            k += S;
+            if (k >= k1) break;
+            a.load(Pi, rows, vals, k + S, k1, R, sub);
+            row_step(b, B, Phi, R, sub, gmask, eps, cur, acc, bc);
+            k += S;
         }
         if (cur != 0xffffffffu)
 #pragma unroll
@@ -519,7 +557,8 @@ altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, co
     while (lpn < 32 && (u64)lpn * ve < R) lpn <<= 1;
     const int ch = (int)((R + (u64)lpn * ve - 1) / ((u64)lpn * ve));  // 1, 2 or 4 (only with 32 lanes)
     const u64 nchunks = (t->nnz + PR_CHUNK - 1) / PR_CHUNK;
-    const int grid = (int)std::max<u64>(1, std::min<u64>((nchunks + 7) / 8, (u64)num_sms() * 8));
+    const int per_sm = ch * ve * (int)fsz <= 16 ? (fsz == 4 ? 4 : 3) : 2;  // pr_min_blocks: one wave
+    const int grid = (int)std::max<u64>(1, std::min<u64>((nchunks + 7) / 8, (u64)num_sms() * per_sm));
     const u64 nnz = t->nnz;
     if (ft == ALTOB_F64) {
         if (vec) launch_phi_rows<double, 2>(lpn, ch, grid, (const double*)dpi, rows, (const double*)svals,

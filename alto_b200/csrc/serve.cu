@@ -62,8 +62,11 @@ static u64 footprint(const altob_request& r)
     const u64 resident = r.nnz * (8 + vsz + 4 * (u64)r.nmode);  // key, value, oidx
     const u64 model = rows * r.rank * fsz * (r.kind == ALTOB_REQ_CP_APR ? 4 : 2) +
                       r.dims[r.nmode - 1] * r.rank * fsz + (u64)r.nmode * r.rank * r.rank * 8 * 2;
-    const u64 pi = r.kind == ALTOB_REQ_CP_APR ? r.nnz * r.rank * fsz : 0;  // precomputed Phi rows
-    return std::max(build_peak, resident + pi) + model + (16ull << 20);
+    const bool apr = r.kind == ALTOB_REQ_CP_APR;
+    const u64 pi = apr ? r.nnz * r.rank * fsz : 0;  // precomputed Khatri-Rao rows
+    // row-ordered Phi stream (row, value, position per mode) and its sort scratch
+    const u64 stream = apr ? r.nnz * ((u64)r.nmode * (8 + fsz) + 24) : 0;
+    return std::max(build_peak, resident + pi + stream) + model + (16ull << 20);
 }
 
 struct Job {
