@@ -480,7 +480,7 @@ struct RecWords {
 inline size_t grouped_smem(int hslots, int mm, size_t fsz, int hot = 0, int R = 0)
 {
     const int rw = (mm + (int)(fsz / 4) + 3) & ~3;
-    size_t b = (size_t)GT_TILE * rw * 4 * 2;  // records, then records in run order
+    size_t b = (size_t)(GT_TILE + GT_TILE + GT_TILE / 32) * rw * 4;  // records, then records in run order (padded)
     b += (size_t)hslots * 8;                  // tags + counts
     b += (size_t)GT_TILE * 4;                 // claimed-slot list
     b += (size_t)hot * 4;                     // hot-row tags
@@ -508,6 +508,13 @@ inline int grouped_hot_slots(int R, size_t fsz)
     while (h * 2 <= 256 && (size_t)(h * 2) * R * fsz <= 16384) h *= 2;
     return h >= 16 ? h : 0;
 }
+
+// Slot of run-ordered record p: one padding record after every 32, so the
+// stretches that the lane groups of a warp read at the same time start in
+// different 16-byte bank groups (unpadded they are 512 bytes apart: one bank
+// group, a 4-way conflict on every record load).
+__device__ __forceinline__ int rslot(int p) { return p + (p >> 5); }
+constexpr int GT_SREC = GT_TILE + GT_TILE / 32;  // run-ordered record slots
 
 template <typename FT, int RW>
 __device__ __forceinline__ void load_rec(const u32* r, u32* w)
@@ -696,8 +703,8 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
     int p = p0;
     for (; p + 1 < pe; p += 2) {
         u32 w0[RW], w1[RW];
-        load_rec<FT, RW>(gs.srec + (size_t)p * RW, w0);
-        load_rec<FT, RW>(gs.srec + (size_t)(p + 1) * RW, w1);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot(p) * RW, w0);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot(p + 1) * RW, w1);
         FT y0[MM - 1][VEC], y1[MM - 1][VEC];
 #pragma unroll
         for (int k = 0; k < MM - 1; ++k) {
@@ -709,7 +716,7 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
     }
     if (p < pe) {
         u32 w0[RW];
-        load_rec<FT, RW>(gs.srec + (size_t)p * RW, w0);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot(p) * RW, w0);
         FT y0[MM - 1][VEC];
 #pragma unroll
         for (int k = 0; k < MM - 1; ++k) vload<FT, VEC>(Ub[k] + (size_t)w0[1 + k] * Ru, y0[k]);
@@ -729,7 +736,7 @@ __device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, in
     GroupedSmem g;
     g.rec = reinterpret_cast<u32*>(smem);
     g.srec = g.rec + (size_t)GT_TILE * RW;
-    g.tag = g.srec + (size_t)GT_TILE * RW;
+    g.tag = g.srec + (size_t)GT_SREC * RW;
     g.cnt = g.tag + H;
     g.used = g.cnt + H;
     g.htag = g.used + GT_TILE;
@@ -947,7 +954,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             const int sl = slv[k];
             const u32 pos = sl >= 0 ? cnt[sl] + rankv[k] : slotted + rankv[k];
             const u32* src = rec + (size_t)it * RW;
-            u32* dst = srec + (size_t)pos * RW;
+            u32* dst = srec + (size_t)rslot((int)pos) * RW;
 #pragma unroll
             for (int w4 = 0; w4 < RW; w4 += 4)
                 *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
@@ -980,7 +987,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     for (; p + GT_NZS - 1 < pend; p += GT_NZS) {
         u32 w[GT_NZS][RW];
 #pragma unroll
-        for (int q = 0; q < GT_NZS; ++q) load_rec<FT, RW>(srec + (size_t)(p + q) * RW, w[q]);
+        for (int q = 0; q < GT_NZS; ++q) load_rec<FT, RW>(srec + (size_t)rslot(p + q) * RW, w[q]);
         FT x[GT_NZS][CH][VEC];
 #pragma unroll
         for (int q = 0; q < GT_NZS; ++q)
@@ -1003,7 +1010,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     }
     for (; p < pend; ++p) {
         u32 w0[RW];
-        load_rec<FT, RW>(srec + (size_t)p * RW, w0);
+        load_rec<FT, RW>(srec + (size_t)rslot(p) * RW, w0);
         FT x0[CH][VEC];
         nz_row<FT, MM, NM, LPN, VEC, CH, PHI>(w0, Uo, Ut, R, sub, nother, a.eps, gmask, x0);
         if (w0[0] != prow) {
