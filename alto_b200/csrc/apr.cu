@@ -226,20 +226,44 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
         }
     } pi_free{nullptr, nullptr, nullptr, nullptr};
     const u64 nnz = t->nnz;
-    const AprPhi kind = nnz ? apr_phi_kind(t, R, sizeof(FT), max_inner) : PHI_OTF;
+    AprPhi kind = nnz ? apr_phi_kind(t, R, sizeof(FT), max_inner) : PHI_OTF;
+    // Memory can go to other streams between the choice and the allocations
+    // (concurrent requests of a server): an allocation that fails falls back
+    // to the next path, which gives the same Phi.
+    auto drop_stream = [&]() {
+        dfree(rows);
+        dfree(inv);
+        dfree(svals);
+        rows = inv = nullptr;
+        svals = nullptr;
+        pi_free.r = pi_free.i = pi_free.v = nullptr;
+    };
     if (kind == PHI_ROWS) {
-        ALTOB_TRY(dmalloc_t(&rows, (size_t)N * nnz));
+        altob_status a = dmalloc_t(&rows, (size_t)N * nnz);
         pi_free.r = rows;
-        ALTOB_TRY(dmalloc_t(&inv, (size_t)N * nnz));
+        if (a == ALTOB_OK) a = dmalloc_t(&inv, (size_t)N * nnz);
         pi_free.i = inv;
-        ALTOB_TRY(dmalloc_t(&svals, (size_t)N * nnz));
+        if (a == ALTOB_OK) a = dmalloc_t(&svals, (size_t)N * nnz);
         pi_free.v = svals;
-        for (int n = 0; n < N; ++n)
-            ALTOB_TRY(mode_order_device(t, n, ft, rows + (size_t)n * nnz, svals + (size_t)n * nnz,
-                                        inv + (size_t)n * nnz, st));
+        for (int n = 0; n < N && a == ALTOB_OK; ++n)
+            a = mode_order_device(t, n, ft, rows + (size_t)n * nnz, svals + (size_t)n * nnz, inv + (size_t)n * nnz,
+                                  st);
+        if (a == ALTOB_ERR_NOMEM) {
+            drop_stream();
+            kind = PHI_PRE;
+        } else if (a != ALTOB_OK) {
+            return a;
+        }
     }
     if (kind != PHI_OTF) {
-        ALTOB_TRY(dmalloc(&pi, nnz * (size_t)R * sizeof(FT)));
+        const altob_status a = dmalloc(&pi, nnz * (size_t)R * sizeof(FT));
+        if (a == ALTOB_ERR_NOMEM) {
+            drop_stream();
+            pi = nullptr;
+            kind = PHI_OTF;
+        } else if (a != ALTOB_OK) {
+            return a;
+        }
         pi_free.p = pi;
     }
     int iter;
