@@ -415,13 +415,14 @@ __global__ void __launch_bounds__(MT_THREADS) k_tiled(TiledArgs<FT> a)
 //
 // Second MTTKRP / Phi kernel: no shared-memory accumulators at all.  Per tile
 // of GT_TILE nonzeros:
-//   A1  load keys and values (coalesced), write one record per nonzero
-//       (mode indices + value) to shared memory, claim a slot for the output
+//   A1  load keys and values (coalesced), form one record per nonzero
+//       (mode indices + value) in registers, claim a slot for the output
 //       row in a direct-mapped tag table, and take a rank inside the slot
 //       with one atomic per group of equal slots in a warp (match_any);
 //   A2  exclusive scan of the slot counts in claim order;
-//   A3  scatter the nonzero numbers into slot order (a counting sort), so
-//       nonzeros with the same output row are contiguous;
+//   A3  write each record once to shared memory at its place in slot order
+//       (a counting sort), so nonzeros with the same output row are
+//       contiguous;
 //   B   each lane group walks a contiguous range of the sorted list, gathers
 //       the other modes' rows, keeps the running sum of equal output rows in
 //       registers and adds each finished run to global memory with one
@@ -453,13 +454,24 @@ __device__ __forceinline__ void prefetch_row(const FT* p, int R)
 #define GT_NZS 2
 #endif
 
-// Launch bounds of the grouped kernels; a build may ask for a minimum number
-// of resident blocks per SM (caps registers) with -DGT_MIN_BLOCKS=n.
-#ifdef GT_MIN_BLOCKS
-#define GT_BOUNDS __launch_bounds__(MT_THREADS, GT_MIN_BLOCKS)
-#else
-#define GT_BOUNDS __launch_bounds__(MT_THREADS)
-#endif
+// Resident blocks per SM that a grouped kernel instance is compiled for (a
+// register cap of 65536 / (256 n); 0: the compiler's own choice).  The
+// kernel is latency-bound: the order-3 FP32 MTTKRP with its records in
+// registers takes 2.88 ms per mode at 4 blocks (64 registers) against 3.27 ms
+// at 3 (the 3-mode Zipf tensor, 100.8M nonzeros, rank 32).  Order 5 (3
+// blocks), the generic-order two-chunk instances (2) and the precomputed-row
+// Phi (4) are held at the occupancy they had with every record staged in
+// shared memory; order 4 reaches 4 blocks uncapped.
+template <typename FT, int NM, int CH, bool PHI>
+constexpr int grouped_min_blocks()
+{
+    if (sizeof(FT) != 4) return 0;
+    if (NM == 0 && CH == 2) return 2;
+    if (CH != 1) return 0;
+    if (NM == 1) return 4;
+    if (PHI) return 0;
+    return NM == 3 ? 4 : NM == 5 ? 3 : 0;
+}
 
 // Record modes of a grouped kernel instance: NM = 3..5 (static order), 0
 // (any order, loops bounded at run time) or 1 (precomputed Khatri-Rao rows:
@@ -480,7 +492,8 @@ struct RecWords {
 inline size_t grouped_smem(int hslots, int mm, size_t fsz, int hot = 0, int R = 0)
 {
     const int rw = (mm + (int)(fsz / 4) + 3) & ~3;
-    size_t b = (size_t)(GT_TILE + GT_TILE + GT_TILE / 32) * rw * 4;  // records, then records in run order (padded)
+    size_t b = (size_t)(GT_TILE + GT_TILE / 32) * rw * 4;  // records in run order (padded)
+    if (rw > 4) b += (size_t)GT_TILE * rw * 4;             // records in stream order
     b += (size_t)hslots * 8;                  // tags + counts
     b += (size_t)GT_TILE * 4;                 // claimed-slot list
     b += (size_t)hot * 4;                     // hot-row tags
@@ -537,8 +550,8 @@ __device__ __forceinline__ FT rec_val(const u32* w)
 }
 
 struct GroupedSmem {
-    u32* rec;
     u32* srec;
+    u32* rec;  // records in stream order (records wider than 4 words only)
     u32* tag;
     u32* cnt;
     u32* used;
@@ -734,9 +747,9 @@ __device__ __forceinline__ GroupedSmem grouped_smem_ptrs(unsigned char* smem, in
 {
     constexpr int RW = RecWords<FT, MM>::n;
     GroupedSmem g;
-    g.rec = reinterpret_cast<u32*>(smem);
-    g.srec = g.rec + (size_t)GT_TILE * RW;
-    g.tag = g.srec + (size_t)GT_SREC * RW;
+    g.srec = reinterpret_cast<u32*>(smem);
+    g.rec = RW > 4 ? g.srec + (size_t)GT_SREC * RW : nullptr;
+    g.tag = g.srec + (size_t)GT_SREC * RW + (RW > 4 ? (size_t)GT_TILE * RW : 0);
     g.cnt = g.tag + H;
     g.used = g.cnt + H;
     g.htag = g.used + GT_TILE;
@@ -773,7 +786,6 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     constexpr int FW = (int)(sizeof(FT) / 4);
     const int R = a.R, H = a.hslots;
     const int nmode = PRE ? 2 : NM ? NM : a.nmode;
-    u32* rec = gs.rec;
     u32* srec = gs.srec;
     u32* tag = gs.tag;
     u32* cnt = gs.cnt;
@@ -811,17 +823,21 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             if (r + 2 < a.key.nrun && a.key.run_start[r + 2] < g0 + (u64)GT_TILE) slow_hi = true;
         }
     }
-    // ---- A1: records [target, others..., value], slot claims, ranks
-    u64 lo[GT_IPT], posv[GT_IPT];
+    // ---- A1: records [target, others..., value], slot claims, ranks.
+    // Records of 4 words stay in registers until A3 writes them once, in run
+    // order; wider ones are staged in shared memory (registers for 4 of them
+    // would cost occupancy).
+    u64 lo[GT_IPT];
+    u32 pv[GT_IPT];  // read position when reading through a permutation
     VT vv[GT_IPT];
 #pragma unroll
     for (int k = 0; k < GT_IPT; ++k) {
         const int it = tid + k * MT_THREADS;
         const u64 g = g0 + it;
-        posv[k] = 0;
+        pv[k] = 0;
         if (it < nvalid) {
-            const u64 pos = a.perm ? (u64)a.perm[g] : g;
-            posv[k] = pos;
+            if (a.perm) pv[k] = a.perm[g];
+            const u64 pos = a.perm ? (u64)pv[k] : g;
             if (!a.perm) {  // the stream is read once: keep L2 for factor rows
                 lo[k] = __ldcs(reinterpret_cast<const unsigned long long*>(a.key.klo) + pos);
                 vv[k] = ldcs_val(vals + pos);
@@ -831,8 +847,14 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             }
         }
     }
+    constexpr bool REGREC = RW == 4;
+    // slot and rank inside the slot (or among the direct nonzeros); packed as
+    // (slot + 2) << 16 | rank when the records are in registers (fewer live
+    // registers there, more in the shared-memory form)
+    u32 slr[GT_IPT];
     int slv[GT_IPT];
     u32 rankv[GT_IPT];
+    u32 rg[GT_IPT][RW];  // the records (static indices only: registers)
 #pragma unroll
     for (int k = 0; k < GT_IPT; ++k) {
         const int it = tid + k * MT_THREADS;
@@ -840,21 +862,20 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
         int sl = -2;
         bool claimed = false;
         u32 h = 0;
+#pragma unroll
+        for (int w = 0; w < RW; ++w) rg[k][w] = 0u;
         if (it < nvalid) {
+            const u64 pos = a.perm ? (u64)pv[k] : g;
             u64 hi;
-            if (a.key.khi) hi = a.key.khi[posv[k]];
+            if (a.key.khi) hi = a.key.khi[pos];
             else if (a.key.nrun == 0) hi = 0;
-            else if (slow_hi) hi = key_hi(a.key, posv[k]);
+            else if (slow_hi) hi = key_hi(a.key, pos);
             else hi = g >= nstart ? hnext : hcur;
-            u32* r = rec + (size_t)it * RW;
-            u32 trow = 0;
-            if constexpr (PRE) {
-                trow = field(lo[k], hi, a.fld.pos[target], a.fld.mask[target]);
-                r[0] = trow;
-                r[1] = (u32)posv[k];
-                // the precomputed row comes from DRAM: start fetching it now
-                prefetch_row<FT>(Uo[0] + (size_t)posv[k] * R, R);
-            } else {
+            if constexpr (!REGREC) {
+                // wide records: each word straight to shared memory (word 0:
+                // the target index; then the other modes in order; the value)
+                u32* r = gs.rec + (size_t)it * RW;
+                u32 trow = 0;
 #pragma unroll
                 for (int m = 0; m < MM; ++m) {
                     if (NM == 0 && m >= nmode) break;
@@ -862,27 +883,87 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
                     r[m == target ? 0 : (m < target ? m + 1 : m)] = c;
                     if (m == target) trow = c;
                 }
-            }
-            const FT fv = (FT)vv[k];
-            if constexpr (FW == 1) {
-                r[MM] = __float_as_uint((float)fv);
+                rg[k][0] = trow;
+                const FT fv = (FT)vv[k];
+                if constexpr (FW == 1) {
+                    r[MM] = __float_as_uint((float)fv);
+                } else {
+                    const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
+                    r[MM] = (u32)b;
+                    r[MM + 1] = (u32)(b >> 32);
+                }
             } else {
-                const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
-                r[MM] = (u32)b;
-                r[MM + 1] = (u32)(b >> 32);
+                if constexpr (PRE) {
+                    rg[k][0] = field(lo[k], hi, a.fld.pos[target], a.fld.mask[target]);
+                    rg[k][1] = (u32)pos;
+                    // the precomputed row comes from DRAM: start fetching it now
+                    prefetch_row<FT>(Uo[0] + (size_t)pos * R, R);
+                } else {
+                    // word 0: the target index; word s >= 1: mode s-1 below
+                    // the target, mode s above it
+                    u32 c[MM];
+#pragma unroll
+                    for (int m = 0; m < MM; ++m)
+                        c[m] = (NM == 0 && m >= nmode) ? 0u : field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
+                    u32 trow = c[0];
+#pragma unroll
+                    for (int m = 1; m < MM; ++m)
+                        if (m == target) trow = c[m];
+                    rg[k][0] = trow;
+#pragma unroll
+                    for (int s = 1; s < MM; ++s) rg[k][s] = s - 1 < target ? c[s - 1] : c[s];
+                }
+                const FT fv = (FT)vv[k];
+                if constexpr (FW == 1) {
+                    rg[k][MM] = __float_as_uint((float)fv);
+                } else {
+                    const unsigned long long b = (unsigned long long)__double_as_longlong((double)fv);
+                    rg[k][MM] = (u32)b;
+                    rg[k][MM + 1] = (u32)(b >> 32);
+                }
             }
             sl = -1;
-            if (H) {
-                h = trow & (u32)(H - 1);
-                const u32 old = atomicCAS(&tag[h], 0u, trow + 1u);
-                if (old == 0u) {
-                    claimed = true;
-                    sl = (int)h;
-                } else if (old == trow + 1u) {
-                    sl = (int)h;
+            h = rg[k][0] & (u32)(H - 1);
+            if constexpr (!REGREC) {
+                if (H) {
+                    const u32 old = atomicCAS(&tag[h], 0u, rg[k][0] + 1u);
+                    if (old == 0u) {
+                        claimed = true;
+                        sl = (int)h;
+                    } else if (old == rg[k][0] + 1u) {
+                        sl = (int)h;
+                    }
                 }
             }
         }
+        u32 peers;
+        if constexpr (REGREC) {
+            // lanes with the same output row form one group (rows are below
+            // 0xffffffff: the tags store row + 1); its first lane claims the
+            // slot for all of them, so a row repeated across the warp (the
+            // head of a skewed mode) costs one compare-and-swap, not one per
+            // nonzero
+            peers = __match_any_sync(0xffffffffu, sl == -2 ? 0xffffffffu : rg[k][0]);
+            const int leader = __ffs(peers) - 1;
+            if (H) {
+                u32 old = 0;
+                if (sl == -1 && lane == leader) old = atomicCAS(&tag[h], 0u, rg[k][0] + 1u);
+                old = __shfl_sync(0xffffffffu, old, leader);
+                if (sl == -1) {
+                    if (old == 0u) {
+                        claimed = lane == leader;
+                        sl = (int)h;
+                    } else if (old == rg[k][0] + 1u) {
+                        sl = (int)h;
+                    }
+                }
+            }
+        } else {
+            // one compare-and-swap per nonzero (above), then groups of equal
+            // slots (fewer registers than grouping first: wide records)
+            peers = __match_any_sync(0xffffffffu, sl >= 0 ? (u32)sl : (0x80000000u | (u32)lane));
+        }
+        const int leader = __ffs(peers) - 1;
         const u32 cm = __ballot_sync(0xffffffffu, claimed);
         if (cm) {
             u32 base = 0;
@@ -890,9 +971,6 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             base = __shfl_sync(0xffffffffu, base, 0);
             if (claimed) used[base + __popc(cm & lt_mask)] = h;
         }
-        const u32 key = sl >= 0 ? (u32)sl : (0x80000000u | (u32)lane);
-        const u32 peers = __match_any_sync(0xffffffffu, key);
-        const int leader = __ffs(peers) - 1;
         u32 base = 0;
         if (sl >= 0 && lane == leader) base = atomicAdd(&cnt[sl], (u32)__popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
@@ -904,8 +982,12 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
             db = __shfl_sync(0xffffffffu, db, 0);
             if (sl == -1) rank = db + __popc(dm & lt_mask);
         }
-        slv[k] = sl;
-        rankv[k] = rank;
+        if constexpr (REGREC) {
+            slr[k] = ((u32)(sl + 2) << 16) | rank;
+        } else {
+            slv[k] = sl;
+            rankv[k] = rank;
+        }
     }
     __syncthreads();
     // ---- A2: exclusive scan of the counts in claim order
@@ -951,13 +1033,18 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     for (int k = 0; k < GT_IPT; ++k) {
         const int it = tid + k * MT_THREADS;
         if (it < nvalid) {
-            const int sl = slv[k];
-            const u32 pos = sl >= 0 ? cnt[sl] + rankv[k] : slotted + rankv[k];
-            const u32* src = rec + (size_t)it * RW;
+            const int sl = REGREC ? (int)(slr[k] >> 16) - 2 : slv[k];
+            const u32 rank = REGREC ? slr[k] & 0xffffu : rankv[k];
+            const u32 pos = sl >= 0 ? cnt[sl] + rank : slotted + rank;
             u32* dst = srec + (size_t)rslot((int)pos) * RW;
+            if constexpr (REGREC) {
+                *reinterpret_cast<uint4*>(dst) = make_uint4(rg[k][0], rg[k][1], rg[k][2], rg[k][3]);
+            } else {
+                const u32* src = gs.rec + (size_t)it * RW;
 #pragma unroll
-            for (int w4 = 0; w4 < RW; w4 += 4)
-                *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
+                for (int w4 = 0; w4 < RW; w4 += 4)
+                    *reinterpret_cast<uint4*>(dst + w4) = *reinterpret_cast<const uint4*>(src + w4);
+            }
         }
     }
     __syncthreads();
@@ -1038,7 +1125,7 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
 }
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void GT_BOUNDS k_grouped(TiledArgs<FT> a)
+__device__ __forceinline__ void grouped_kernel_body(const TiledArgs<FT>& a)
 {
     constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1060,6 +1147,18 @@ __global__ void GT_BOUNDS k_grouped(TiledArgs<FT> a)
     }
 }
 
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped(TiledArgs<FT> a)
+{
+    grouped_kernel_body<FT, VT, NM, LPN, VEC, CH, PHI>(a);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI, int MINB>
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_grouped_mb(TiledArgs<FT> a)
+{
+    grouped_kernel_body<FT, VT, NM, LPN, VEC, CH, PHI>(a);
+}
+
 // Batched form: the tiles of many tensors (one TiledArgs each, same shape
 // class and slot count) in one persistent launch.  tile_prefix[b] is the
 // first global tile of tensor b; tensors whose active flag is 0 are skipped.
@@ -1075,7 +1174,7 @@ struct BatchTiles {
 };
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void GT_BOUNDS k_grouped_batch(BatchTiles<FT> bt)
+__device__ __forceinline__ void grouped_batch_body(const BatchTiles<FT>& bt)
 {
     constexpr int MM = grouped_mm<NM>();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1092,6 +1191,18 @@ __global__ void GT_BOUNDS k_grouped_batch(BatchTiles<FT> bt)
         if (!bt.active[bt.bid[lo]]) continue;
         grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(bt.args[lo], gt - bt.tile_prefix[lo], gs);
     }
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
+{
+    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI, int MINB>
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_grouped_batch_mb(BatchTiles<FT> bt)
+{
+    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
 }
 
 template <typename FT>

@@ -56,7 +56,11 @@ template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
 altob_status launch_grouped(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     static std::atomic<size_t> configured{0};
-    return launch_kernel(k_grouped<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
+    constexpr int mb = grouped_min_blocks<FT, NM, CH, PHI>();
+    if constexpr (mb > 0)
+        return launch_kernel(k_grouped_mb<FT, VT, NM, LPN, VEC, CH, PHI, mb>, configured, &a, c, st, bps);
+    else
+        return launch_kernel(k_grouped<FT, VT, NM, LPN, VEC, CH, PHI>, configured, &a, c, st, bps);
 }
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
@@ -104,7 +108,11 @@ template <typename FT, typename VT, int NM, int LPN, int VEC, int CH>
 altob_status launch_batch_one(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     static std::atomic<size_t> configured{0};
-    return launch_kernel(k_grouped_batch<FT, VT, NM, LPN, VEC, CH, false>, configured, &bt, c, st, bps);
+    constexpr int mb = grouped_min_blocks<FT, NM, CH, false>();
+    if constexpr (mb > 0)
+        return launch_kernel(k_grouped_batch_mb<FT, VT, NM, LPN, VEC, CH, false, mb>, configured, &bt, c, st, bps);
+    else
+        return launch_kernel(k_grouped_batch<FT, VT, NM, LPN, VEC, CH, false>, configured, &bt, c, st, bps);
 }
 
 template <typename FT, typename VT, int NM>
