@@ -685,9 +685,12 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
 {
     constexpr int RW = RecWords<FT, MM>::n;
     const u32 Ru = (u32)R;
+    // Lanes past the rank (R below LPN * VEC) load the row's last elements,
+    // so every load stays inside its row; flush_run writes only r0 < R.
+    const int col = min(sub * VEC, R - VEC);
     const FT* Ub[MM - 1];
 #pragma unroll
-    for (int k = 0; k < MM - 1; ++k) Ub[k] = Uo[k] + sub * VEC;
+    for (int k = 0; k < MM - 1; ++k) Ub[k] = Uo[k] + col;
     u32 cur = 0xffffffffu;
     int len = 0;
     FT acc[1][VEC];
