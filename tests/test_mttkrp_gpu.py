@@ -78,6 +78,35 @@ def test_gpu_mttkrp_fp32_against_fp64(oracle, case):
         assert rel_fro(dU[mode].cpu().numpy(), want_mode) < TOL32
 
 
+@pytest.mark.parametrize("rank", [12, 24])
+def test_gpu_mttkrp_lanes_past_rank(oracle, rank):
+    """Ranks that leave lanes of a nonzero's lane group past the rank (12 and
+    24: 4 or 8 lanes of 4 FP32 values, 8 or 16 lanes of 2 FP64 values, the
+    last ones beyond R); their loads stay in the row and nothing they hold is
+    written, in FP64 (+= semantics) and FP32 (overwrite)."""
+    torch = pytest.importorskip("torch")
+    dims, nnz, nprtn = (300, 200, 100), 40_000, 8
+    dims_a, cidx, vals = synth.uniform_distinct(dims, nnz, seed=rank)
+    at = ab.create_alto(_coo(dims_a, cidx, vals), nprtn, 0)
+    ot = oracle.create(dims_a, cidx, vals, nprtn, at.info()["lit_bits"])
+    at32 = ab.create_alto(_coo(dims_a, cidx, vals), nprtn, 0, val_dtype="f32")
+    ot32 = oracle.create(dims_a, cidx, vals.astype(np.float32).astype(np.float64), nprtn, at32.info()["lit_bits"])
+    for mode in range(len(dims)):
+        U = synth.random_factors(dims_a, rank, seed=mode)
+        want = [u.copy() for u in U]
+        ot.mttkrp(mode, want, rank)
+        dU = [torch.from_numpy(u).cuda() for u in U]
+        ab.mttkrp_alto_par(mode, dU, rank, at)
+        assert rel_fro(dU[mode].cpu().numpy(), want[mode]) < TOL64, (rank, mode)
+        U32 = [u.astype(np.float32) for u in U]
+        want32 = [u.astype(np.float64) for u in U32]
+        ot32.mttkrp(mode, want32, rank)
+        d32 = [torch.from_numpy(u).cuda() for u in U32]
+        ab.mttkrp_alto_par(mode, d32, rank, at32, accumulate=False)
+        got32 = d32[mode].cpu().numpy()
+        assert rel_fro(got32, want32[mode] - U32[mode].astype(np.float64)) < TOL32, (rank, mode)
+
+
 def test_gpu_mttkrp_zipf_skew_fp64_and_fp32(oracle):
     """Config-2 shape (Zipf 1.1 skew, 65-bit keys) at reduced size."""
     torch = pytest.importorskip("torch")
