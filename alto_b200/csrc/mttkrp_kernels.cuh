@@ -828,8 +828,8 @@ __device__ __forceinline__ void grouped_tile(const TiledArgs<FT>& a, u64 ti, con
     }
     // ---- A1: records [target, others..., value], slot claims, ranks.
     // Records of 4 words stay in registers until A3 writes them once, in run
-    // order; wider ones are staged in shared memory (registers for 4 of them
-    // would cost occupancy).
+    // order; wider ones are staged in shared memory (a thread's GT_IPT wide
+    // records held in registers would cost occupancy).
     u64 lo[GT_IPT];
     u32 pv[GT_IPT];  // read position when reading through a permutation
     VT vv[GT_IPT];
