@@ -240,6 +240,23 @@ class RefLib:
                        _ptr_array(U), _p(lam, _f64p), _p(s, _f64p))
         return U, lam, dict(loglik=s[0], fit=s[1], kkt=s[2], outer=int(s[3]), inner=int(s[4]))
 
+    def read(self, path, binary=False, zero_based=0):
+        """The reference's ImportSparseTensor: (dims, cidx (modes x nnz), vals)."""
+        L = self.L
+        L.ref_read_open.restype = C.c_void_p
+        L.ref_read_open.argtypes = [C.c_char_p, C.c_int, C.c_uint64, _i32p, _u64p]
+        L.ref_read_take.restype = None
+        L.ref_read_take.argtypes = [C.c_void_p, _u64p, _u64p, _f64p]
+        nm = np.zeros(1, np.int32)
+        nnz = np.zeros(1, np.uint64)
+        h = L.ref_read_open(path.encode(), int(bool(binary)), int(zero_based), _p(nm, _i32p), _p(nnz, _u64p))
+        n, z = int(nm[0]), int(nnz[0])
+        dims = np.zeros(n, np.uint64)
+        cidx = np.zeros((n, z), np.uint64)
+        vals = np.zeros(z)
+        L.ref_read_take(h, _p(dims, _u64p), _p(cidx, _u64p), _p(vals, _f64p))
+        return dims, cidx, vals
+
     def bench_mttkrp(self, dims, cidx, vals, nprtn, lit_bits, rank, iters, seed):
         dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)
         cs = np.zeros(1)

@@ -21,6 +21,7 @@
 #include "cpd.hpp"
 #include "apr.hpp"
 
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -232,6 +233,32 @@ double run_bench(SparseTensor* X, int nprtn, uint64_t rank, int iters,
 extern "C" {
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
+
+// The reference's file reader, ImportSparseTensor (src/sptensor.cpp:165-258,
+// text format :75-161): ref_read_open reads the file (the path must name a
+// readable file; the reference asserts otherwise) and reports its order and
+// nonzero count; ref_read_take copies dims, the mode-major coordinates and
+// the values out and frees the tensor.
+void* ref_read_open(const char* path, int binary, uint64_t zero_based, int* nmode, uint64_t* nnz)
+{
+    SparseTensor* X = nullptr;
+    ImportSparseTensor(path, binary ? BINARY_FORMAT : TEXT_FORMAT, &X, (IType)zero_based);
+    *nmode = X->nmodes;
+    *nnz = X->nnz;
+    return X;
+}
+
+void ref_read_take(void* p, uint64_t* dims, uint64_t* cidx, double* vals)
+{
+    SparseTensor* X = static_cast<SparseTensor*>(p);
+    const uint64_t nnz = X->nnz;
+    for (int n = 0; n < X->nmodes; ++n) {
+        dims[n] = X->dims[n];
+        memcpy(cidx + (size_t)n * nnz, X->cidx[n], nnz * sizeof(uint64_t));
+    }
+    memcpy(vals, X->vals, nnz * sizeof(double));
+    DestroySparseTensor(X);
+}
 
 int ref_create_dump(int nmode, const uint64_t* dims, uint64_t nnz,
                     const uint64_t* cidx, const double* vals, int nprtn,

@@ -79,6 +79,38 @@ def test_tns_reader_large_parallel(tmp_path):
     np.testing.assert_allclose(Y.vals, vals, rtol=1e-5)  # %g keeps 6 digits
 
 
+def test_readers_match_the_reference_reader(tmp_path):
+    """altob_read_tns / altob_read_bin against the reference's own
+    ImportSparseTensor (src/sptensor.cpp:75-258, compiled under oracle/_ref):
+    the same dims, coordinates and values, bit for bit, for the rule cases
+    (comments, empty lines, tabs, 1- and 0-based) and generated files."""
+    from alto_b200 import synth
+    from oracle.orc import RefLib, ref_available
+    if not ref_available():
+        pytest.skip("reference library not built")
+    ref = RefLib()
+    rules = str(tmp_path / "r.tns")
+    with open(rules, "w") as f:
+        f.write("# a comment\n\n1 2 3 1.0\n4\t1 1 2.5\n\n2 2 7 -1e2\n")
+    files = [(rules, False, 0), (rules, False, 1)]
+    for k, (shape, nnz) in enumerate([((300, 200, 100), 200_000), ((50, 40, 30, 20, 7), 30_000)]):
+        dims, cidx, vals = synth.uniform_distinct(shape, nnz, seed=11 + k)
+        X = ab.SparseTensor.from_arrays(dims, cidx, vals)
+        for binary in (False, True):
+            p = str(tmp_path / (f"g{k}." + ("bin" if binary else "tns")))
+            ab.ExportSparseTensor(p, ab.BINARY_FORMAT if binary else ab.TEXT_FORMAT, X)
+            files.append((p, binary, 0))
+    for p, binary, zb in files:
+        rd, rc, rv = ref.read(p, binary=binary, zero_based=zb)
+        if binary:
+            Y = ab.ImportSparseTensor(p, ab.BINARY_FORMAT)
+        else:
+            Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT, zero_based=zb)
+        np.testing.assert_array_equal(Y.dims, rd, err_msg=p)
+        np.testing.assert_array_equal(Y.cidx, rc, err_msg=p)
+        np.testing.assert_array_equal(Y.vals, rv, err_msg=p)
+
+
 def test_binary_round_trip_and_errors(tmp_path):
     dims = np.array([7, 8], np.uint64)
     cidx = np.array([[1, 6], [7, 0]], np.uint64)
