@@ -257,6 +257,14 @@ class RefLib:
         L.ref_read_take(h, _p(dims, _u64p), _p(cidx, _u64p), _p(vals, _f64p))
         return dims, cidx, vals
 
+    def write(self, path, dims, cidx, vals, binary=False):
+        """The reference's ExportSparseTensor of a COO tensor (cidx: modes x nnz)."""
+        L = self.L
+        L.ref_write.restype = None
+        L.ref_write.argtypes = [C.c_char_p, C.c_int, C.c_int, _u64p, C.c_uint64, _u64p, _f64p]
+        dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)
+        L.ref_write(path.encode(), int(bool(binary)), nm, _p(dims, _u64p), nnz, _p(cidx, _u64p), _p(vals, _f64p))
+
     def bench_mttkrp(self, dims, cidx, vals, nprtn, lit_bits, rank, iters, seed):
         dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)
         cs = np.zeros(1)

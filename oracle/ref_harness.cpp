@@ -248,6 +248,15 @@ void* ref_read_open(const char* path, int binary, uint64_t zero_based, int* nmod
     return X;
 }
 
+// The reference's writer, ExportSparseTensor (src/sptensor.cpp:23-70).
+void ref_write(const char* path, int binary, int nmode, const uint64_t* dims, uint64_t nnz,
+               const uint64_t* cidx, const double* vals)
+{
+    SparseTensor* X = make_spt(nmode, dims, nnz, cidx, vals);
+    ExportSparseTensor(path, binary ? BINARY_FORMAT : TEXT_FORMAT, X);
+    DestroySparseTensor(X);
+}
+
 void ref_read_take(void* p, uint64_t* dims, uint64_t* cidx, double* vals)
 {
     SparseTensor* X = static_cast<SparseTensor*>(p);

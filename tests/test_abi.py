@@ -109,6 +109,24 @@ def test_readers_match_the_reference_reader(tmp_path):
         np.testing.assert_array_equal(Y.dims, rd, err_msg=p)
         np.testing.assert_array_equal(Y.cidx, rc, err_msg=p)
         np.testing.assert_array_equal(Y.vals, rv, err_msg=p)
+    # files written by the reference's ExportSparseTensor (src/sptensor.cpp:23-70)
+    dims, cidx, vals = synth.uniform_distinct((300, 200, 100), 50_000, seed=7)
+    p = str(tmp_path / "ref.tns")
+    ref.write(p, dims, cidx, vals)
+    rd, rc, rv = ref.read(p)
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.dims, rd)
+    np.testing.assert_array_equal(Y.cidx, rc)
+    np.testing.assert_array_equal(Y.vals, rv)
+    # its binary writer stores the 4-byte mode count as 8 bytes, the upper 4
+    # being struct padding (src/sptensor.cpp:59): the reference's own reader
+    # can then abort on its mode-count assert, so only this reader reads it
+    p = str(tmp_path / "ref.bin")
+    ref.write(p, dims, cidx, vals, binary=True)
+    Y = ab.ImportSparseTensor(p, ab.BINARY_FORMAT)
+    np.testing.assert_array_equal(Y.dims, dims)
+    np.testing.assert_array_equal(Y.cidx, cidx)
+    np.testing.assert_array_equal(Y.vals, vals)
 
 
 def test_binary_round_trip_and_errors(tmp_path):
