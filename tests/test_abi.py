@@ -129,6 +129,48 @@ def test_readers_match_the_reference_reader(tmp_path):
     np.testing.assert_array_equal(Y.vals, vals)
 
 
+ODD_TNS = {
+    "crlf": "1 2 3 1.0\r\n2 1 1 2.0\r\n",
+    "multi_space": "1  2   3 1.0\n2 1 1   2.0\n",
+    "leading_space": " 1 2 3 1.0\n 2 1 1 2.0\n",
+    "tabs": "1\t2\t3\t1.0\n2\t1\t1\t2.0\n",
+    "no_final_newline": "1 2 3 1.0\n2 1 1 2.0",
+    "exponents": "1 2 3 1e-300\n2 1 1 -2.5E+10\n",
+    "comment_between": "1 2 3 1.0\n# c\n2 1 1 2.0\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(ODD_TNS))
+def test_tns_odd_formatting_matches_the_reference_reader(tmp_path, name):
+    """Line endings, repeated and leading separators, a missing final newline,
+    exponents and comments between data lines read as the reference reads
+    them (src/sptensor.cpp:75-161)."""
+    from oracle.orc import RefLib, ref_available
+    if not ref_available():
+        pytest.skip("reference library not built")
+    p = str(tmp_path / "odd.tns")
+    with open(p, "w", newline="") as f:
+        f.write(ODD_TNS[name])
+    rd, rc, rv = RefLib().read(p)
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.dims, rd)
+    np.testing.assert_array_equal(Y.cidx, rc)
+    np.testing.assert_array_equal(Y.vals, rv)
+
+
+def test_tns_trailing_whitespace(tmp_path):
+    """A separator before the newline: the reference counts the newline as
+    one more token (one mode too many, every value read as 0); this reader
+    ignores trailing whitespace."""
+    p = str(tmp_path / "trail.tns")
+    with open(p, "w") as f:
+        f.write("1 2 3 1.0 \n2 1 1 2.0\t\n")
+    Y = ab.ImportSparseTensor(p, ab.TEXT_FORMAT)
+    np.testing.assert_array_equal(Y.dims, [2, 2, 3])
+    np.testing.assert_array_equal(Y.cidx, [[0, 1], [1, 0], [2, 0]])
+    np.testing.assert_array_equal(Y.vals, [1.0, 2.0])
+
+
 def test_binary_round_trip_and_errors(tmp_path):
     dims = np.array([7, 8], np.uint64)
     cidx = np.array([[1, 6], [7, 0]], np.uint64)
