@@ -82,17 +82,47 @@ altob_status tensor_hotbuf(altob_tensor* t, size_t bytes, void** out)
     return ALTOB_OK;
 }
 
+static bool capturing(cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+altob_status tensor_enter(altob_tensor* t, cudaStream_t st)
+{
+    if (!t->use_ev || t->use_stream == st || capturing(st)) return ALTOB_OK;
+    ALTOB_CUDA(cudaStreamWaitEvent(st, t->use_ev, 0));
+    return ALTOB_OK;
+}
+
+altob_status tensor_leave(altob_tensor* t, cudaStream_t st)
+{
+    if (capturing(st)) return ALTOB_OK;
+    if (!t->use_ev) ALTOB_CUDA(cudaEventCreateWithFlags(&t->use_ev, cudaEventDisableTiming));
+    ALTOB_CUDA(cudaEventRecord(t->use_ev, st));
+    t->use_stream = st;
+    return ALTOB_OK;
+}
+
+// SM count of the current device, cached per device ordinal.
 int num_sms()
 {
-    static int sms = 0;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        int dev = 0;
-        cudaGetDevice(&dev);
+    static std::mutex mu;
+    static std::vector<int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= (int)cache.size()) cache.resize(dev + 1, 0);
+    if (cache[dev] <= 0) {
+        int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    });
-    return sms;
+        cache[dev] = sms > 0 ? sms : 148;
+    }
+    return cache[dev];
 }
 
 // ------------------------------------------------------------ masks
@@ -952,12 +982,17 @@ altob_status altob_destroy(altob_tensor* t)
     // already issued on blocking streams; work on non-blocking streams that
     // uses the tensor must be finished by the caller first
     StreamScope scope(0);
+    if (t->use_ev) {  // after the last call that used the handle, on any stream
+        cudaStreamWaitEvent(0, t->use_ev, 0);
+        cudaEventDestroy(t->use_ev);
+    }
     dfree(t->d_klo);
     dfree(t->d_khi);
     dfree(t->d_run_start);
     dfree(t->d_run_val);
     dfree(t->d_vals);
     for (int n = 0; n < ALTOB_MAX_MODES; ++n) dfree(t->d_oidx[n]);
+    for (int n = 0; n < ALTOB_MAX_MODES; ++n) dfree(t->d_plan[n]);
     dfree(t->scratch);
     dfree(t->hotbuf);
     delete t;
@@ -989,6 +1024,11 @@ altob_status altob_get_info(const altob_tensor* t, altob_info* o)
     o->device_bytes = t->device_bytes;
     o->key_bytes = t->d_khi ? 16 : 8;
     o->nruns = t->nrun;
+    for (int n = 0; n < t->nmode; ++n)
+        if (t->d_plan[n]) {
+            o->plan_modes |= 1 << n;
+            o->plan_bytes += t->nnz * sizeof(uint16_t);
+        }
     return ALTOB_OK;
 }
 

@@ -211,6 +211,12 @@ struct altob_tensor {
     // per-CTA hot-row accumulators of the grouped kernel (grown on demand)
     void* hotbuf = nullptr;
     size_t hotbuf_bytes = 0;
+    // tile plans of the planned MTTKRP kernel, one per mode (built on first use)
+    uint16_t* d_plan[ALTOB_MAX_MODES] = {nullptr};
+    // the stream of the last call that used the cached buffers or plans, and
+    // an event recorded there: a call on another stream waits for it first
+    cudaEvent_t use_ev = nullptr;
+    cudaStream_t use_stream = nullptr;
 };
 
 namespace altob {
@@ -250,6 +256,19 @@ void dfree(void* p);
 // across calls on the same handle.
 altob_status tensor_scratch(altob_tensor* t, size_t bytes, void** out);
 altob_status tensor_hotbuf(altob_tensor* t, size_t bytes, void** out);
+
+// Stream ordering of a handle's shared state (scratch, hot-row buffers, tile
+// plans): tensor_enter makes stream st wait for the last call that used the
+// handle on a different stream; tensor_leave records that this call's work
+// was issued on st.  Both do nothing while st is being captured.
+altob_status tensor_enter(altob_tensor* t, cudaStream_t st);
+altob_status tensor_leave(altob_tensor* t, cudaStream_t st);
+struct TensorUse {
+    altob_tensor* t;
+    cudaStream_t st;
+    TensorUse(altob_tensor* t_, cudaStream_t st_) : t(t_), st(st_) {}
+    ~TensorUse() { if (t) tensor_leave(t, st); }
+};
 
 int num_sms();
 

@@ -89,6 +89,24 @@ static altob_status set_hot_acc(altob_tensor* t, TiledArgs<FT>& a, unsigned grid
     return ALTOB_OK;
 }
 
+// Tile plan of `mode` (k_tile_plan), built on the first call that needs it.
+// Returns false (and leaves no plan) when the 2 bytes per nonzero cannot be
+// allocated; the caller then runs the grouped kernel.
+static bool ensure_plan(altob_tensor* t, int mode, cudaStream_t st)
+{
+    if (t->d_plan[mode]) return true;
+    void* p = nullptr;
+    if (dmalloc(&p, (size_t)t->nnz * sizeof(uint16_t)) != ALTOB_OK) return false;
+    const u64 ntiles = (t->nnz + PT_TILE - 1) / PT_TILE;
+    k_tile_plan<PT_TILE><<<(unsigned)ntiles, PT_TILE / 2, 0, st>>>(key_src(t), t->fld, t->nnz, mode, (u16*)p);
+    if (cudaGetLastError() != cudaSuccess) {
+        dfree(p);
+        return false;
+    }
+    t->d_plan[mode] = (uint16_t*)p;
+    return true;
+}
+
 template <typename FT, typename VT>
 static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, void* dout, u64 R, bool phi,
                                  double eps, const u32* perm, bool cache, cudaStream_t st)
@@ -97,6 +115,10 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     for (int m = 0; m < t->nmode; ++m) aligned = aligned && ptr_aligned16(dU[m]);
     TiledPlan pl;
     ALTOB_TRY(plan_tiled(t, R, sizeof(FT), aligned, cache, &pl));
+    // MTTKRP of a static order 3-5 in ALTO order with one vector chunk per
+    // lane: the planned kernel (ALTOB_PLAN=0 keeps the grouped kernel)
+    const bool planned = pl.grouped && !phi && !perm && cache && t->nmode >= 3 && t->nmode <= 5 && pl.vec > 1 &&
+                         pl.ch == 1 && t->nnz < (1ull << 32) && env_int("ALTOB_PLAN", 1) && ensure_plan(t, mode, st);
     TiledArgs<FT> a;
     memset(&a, 0, sizeof(a));
     a.key = key_src(t);
@@ -123,6 +145,26 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
     c.smem = pl.smem;
     c.grid = dim3(0);
     int bps = 0;
+    if (planned) {
+        a.plan = t->d_plan[mode];
+        a.tile = PT_TILE;
+        a.ntiles = (t->nnz + PT_TILE - 1) / PT_TILE;
+        a.hslots = 0;
+        // FP32 ranks that are a multiple of 8 with 32-byte aligned factors:
+        // 256-bit row pieces, R / 8 lanes per nonzero (ALTOB_VEC8=0: 128-bit)
+        bool al32 = ((uintptr_t)dout & 31u) == 0;
+        for (int m = 0; m < t->nmode; ++m) al32 = al32 && ((uintptr_t)dU[m] & 31u) == 0;
+        if (sizeof(FT) == 4 && R % 8 == 0 && R <= 128 && al32 && env_int("ALTOB_VEC8", 1)) {
+            c.vec = 8;
+            c.lpn = std::max(1, next_pow2((int)(R / 8)));
+        }
+        c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn);
+        ALTOB_TRY((launch_planned<FT, VT>(a, c, st, &bps)));
+        if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned MTTKRP kernel does not fit on an SM");
+        c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, (u64)bps * num_sms())));
+        ALTOB_TRY(set_hot_acc(t, a, c.grid.x, st));
+        return launch_planned<FT, VT>(a, c, st, nullptr);
+    }
     ALTOB_TRY((launch_tiled<FT, VT>(a, c, st, &bps)));
     if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "MTTKRP kernel does not fit on an SM");
     u64 cap = (u64)bps * num_sms();
@@ -187,6 +229,8 @@ altob_status mttkrp_device(altob_tensor* t, int mode, altob_dtype ft, void* cons
     for (int m = 0; m < t->nmode; ++m)
         if (!dU[m]) return fail(ALTOB_ERR_ARG, "a factor pointer is NULL");
     const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_TRY(tensor_enter(t, st));
+    TensorUse use(t, st);
     if (!accumulate) ALTOB_CUDA(cudaMemsetAsync(dU[mode], 0, t->dims[mode] * R * fsz, st));
     if (t->nnz == 0) return ALTOB_OK;
     algo = resolve_algo(t, mode, algo);
@@ -214,6 +258,8 @@ altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* 
     if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
     if (ft != ALTOB_F64 && ft != ALTOB_F32) return fail(ALTOB_ERR_ARG, "compute dtype must be F64 or F32");
     const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_TRY(tensor_enter(t, st));
+    TensorUse use(t, st);
     ALTOB_CUDA(cudaMemsetAsync(dphi, 0, t->dims[mode] * R * fsz, st));
     if (t->nnz == 0) return ALTOB_OK;
     return ft == ALTOB_F64 ? run_tiled<double>(t, mode, dU, dphi, R, true, eps, nullptr, true, st)
@@ -625,6 +671,8 @@ altob_status phi_pre_device(altob_tensor* t, int mode, altob_dtype ft, const voi
     if (!t || !dpi || !dB || !dphi) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
     const size_t fsz = ft == ALTOB_F64 ? 8 : 4;
+    ALTOB_TRY(tensor_enter(t, st));
+    TensorUse use(t, st);
     ALTOB_CUDA(cudaMemsetAsync(dphi, 0, t->dims[mode] * R * fsz, st));
     if (t->nnz == 0) return ALTOB_OK;
     const bool f64 = ft == ALTOB_F64;

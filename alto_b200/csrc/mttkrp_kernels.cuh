@@ -1,29 +1,24 @@
 // mttkrp_kernels.cuh -- MTTKRP and CP-APR Phi kernels on the ALTO stream.
 //
-// Reference kernels replaced (IntelLabs/ALTO):
-//   mttkrp_alto_da_mem_pull   include/alto.hpp:1227-1318  -> k_tiled<..., PHI=false>
-//   mttkrp_alto_op_sched      include/alto.hpp:1320-1415  -> k_tiled reading through oidx
-//   mttkrp_alto_atomic        include/alto.hpp:1030-1088  -> k_tiled without row cache
+// Reference kernels replaced (IntelLabs/ALTO) and the kernel that runs them:
+//   mttkrp_alto_da_mem_pull   include/alto.hpp:1227-1318  -> k_planned (mttkrp_planned.cuh),
+//                                                            k_grouped without a tile plan
+//   mttkrp_alto_op_sched      include/alto.hpp:1320-1415  -> k_grouped reading through oidx
+//   mttkrp_alto_atomic        include/alto.hpp:1030-1088  -> k_grouped without row slots
 //   mttkrp_alto_atomic_cr     include/alto.hpp:1090-1158  -> k_atomic_cr
-//   CalculatePhi_alto_*       include/apr.hpp:383-848     -> k_tiled<..., PHI=true>
+//   CalculatePhi_alto_*       include/apr.hpp:383-848     -> k_grouped<..., PHI=true>
+//   batched MTTKRP (no counterpart)                       -> k_grouped_batch
 //
-// k_tiled: a persistent CTA walks tiles of `tile` consecutive nonzeros of
-// the ALTO-ordered stream (the GPU analogue of the reference's line
-// segments).
-//   Phase A, one thread per nonzero: coalesced loads of key and value, mode
-//     indices read as bit fields, and a shared-memory accumulator row claimed
-//     for the output index (direct-mapped on its low bits; claims are
-//     appended to a list with one atomic per warp).
-//   Phase B, LPN lanes per nonzero with VEC elements each (16-byte loads):
-//     gather the other modes' factor rows, form val * (Khatri-Rao row) (or
-//     the Phi row), add into the claimed row; a nonzero whose slot belongs to
-//     another index goes straight to global memory with a vector atomic.
-//     Lane group q adds its VEC elements in the order rotated by q, so the
-//     NPW groups of a warp hit disjoint shared-memory banks.
-//   Phase C: every claimed row is flushed once with vector atomics and
-//     cleared.
-// The tile is the segment and the flush is the pull of the reference's
-// da_mem_pull; only rows touched by several tiles meet in global memory.
+// k_grouped (below, the default when no tile plan exists): a persistent CTA
+// walks tiles of 1024 consecutive nonzeros of the ALTO-ordered stream (the
+// GPU analogue of the reference's line segments), sorts each tile's records
+// by output row in shared memory (slot claims, a scan, a counting-sort
+// scatter), and lane groups walk runs of equal output rows keeping their sums
+// in registers, one vector atomic per run (the reference's pull reduction).
+// k_planned does the same with the tile order precomputed per mode.
+//
+// k_tiled (kept as an alternative: ALTOB_KERNEL other than 4): per-tile shared-memory
+// accumulator rows claimed by output index, flushed once per tile.
 #pragma once
 
 #include "internal.cuh"
@@ -43,15 +38,28 @@ template <>
 struct VecT<double, 1> { typedef double T; };
 template <>
 struct VecT<double, 2> { typedef double2 T; };
+// 256-bit rows pieces of sm_100 (ld.global.v8.f32): 8 floats per lane
+struct __align__(32) float8_t {
+    float v[8];
+};
+template <>
+struct VecT<float, 8> { typedef float8_t T; };
 
 template <typename FT, int VEC>
 __device__ __forceinline__ void vload(const FT* p, FT* x)
 {
-    typedef typename VecT<FT, VEC>::T V;
-    V v = __ldg(reinterpret_cast<const V*>(p));
-    const FT* f = reinterpret_cast<const FT*>(&v);
+    if constexpr (sizeof(FT) == 4 && VEC == 8) {  // one 256-bit load (sm_100)
+        float* f = reinterpret_cast<float*>(x);
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
+            : "l"(p));
+    } else {
+        typedef typename VecT<FT, VEC>::T V;
+        V v = __ldg(reinterpret_cast<const V*>(p));
+        const FT* f = reinterpret_cast<const FT*>(&v);
 #pragma unroll
-    for (int e = 0; e < VEC; ++e) x[e] = f[e];
+        for (int e = 0; e < VEC; ++e) x[e] = f[e];
+    }
 }
 
 template <typename FT, int VEC>
@@ -91,6 +99,9 @@ __device__ __forceinline__ void gred(FT* p, const FT* x)
 {
     if constexpr (sizeof(FT) == 4 && VEC == 4) {
         atomicAdd(reinterpret_cast<float4*>(p), make_float4(x[0], x[1], x[2], x[3]));
+    } else if constexpr (sizeof(FT) == 4 && VEC == 8) {  // no 256-bit reduction: two 128-bit ones
+        atomicAdd(reinterpret_cast<float4*>(p), make_float4(x[0], x[1], x[2], x[3]));
+        atomicAdd(reinterpret_cast<float4*>(p + 4), make_float4(x[4], x[5], x[6], x[7]));
     } else {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) atomicAdd(p + e, x[e]);
@@ -165,6 +176,7 @@ struct TiledArgs {
     Fields fld;
     int hot;       // per-CTA hot-row slots (power of two; 0: none), grouped kernel only
     FT* hot_acc;   // gridDim.x x hot x R accumulators, one private region per CTA
+    const uint16_t* plan;  // tile plan of the target mode (planned kernel only)
 };
 
 // Dynamic shared-memory bytes of k_tiled.
@@ -527,6 +539,10 @@ inline int grouped_hot_slots(int R, size_t fsz)
 // different 16-byte bank groups (unpadded they are 512 bytes apart: one bank
 // group, a 4-way conflict on every record load).
 __device__ __forceinline__ int rslot(int p) { return p + (p >> 5); }
+// The same with one padding record after every 2^PSH (stretches of 2^PSH
+// records per lane group).
+template <int PSH>
+__device__ __forceinline__ int rslot_t(int p) { return p + (p >> PSH); }
 constexpr int GT_SREC = GT_TILE + GT_TILE / 32;  // run-ordered record slots
 
 template <typename FT, int RW>
@@ -679,7 +695,7 @@ __device__ __forceinline__ void run_add(FT (*racc)[VEC], FT (*x)[VEC])
 // generic loop, written so that the per-nonzero work is the record load, the
 // row loads with 32-bit-operand address products, the products and the run
 // test (23% fewer instructions and 28% less time on the 3-mode Zipf tensor).
-template <typename FT, int MM, int LPN, int VEC>
+template <typename FT, int MM, int LPN, int VEC, int PSH = 5>
 __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedSmem& gs, const FT* const* Uo,
                                           int p0, int pe, int R, int sub, unsigned gmask)
 {
@@ -719,8 +735,8 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
     int p = p0;
     for (; p + 1 < pe; p += 2) {
         u32 w0[RW], w1[RW];
-        load_rec<FT, RW>(gs.srec + (size_t)rslot(p) * RW, w0);
-        load_rec<FT, RW>(gs.srec + (size_t)rslot(p + 1) * RW, w1);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot_t<PSH>(p) * RW, w0);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot_t<PSH>(p + 1) * RW, w1);
         FT y0[MM - 1][VEC], y1[MM - 1][VEC];
 #pragma unroll
         for (int k = 0; k < MM - 1; ++k) {
@@ -732,7 +748,7 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
     }
     if (p < pe) {
         u32 w0[RW];
-        load_rec<FT, RW>(gs.srec + (size_t)rslot(p) * RW, w0);
+        load_rec<FT, RW>(gs.srec + (size_t)rslot_t<PSH>(p) * RW, w0);
         FT y0[MM - 1][VEC];
 #pragma unroll
         for (int k = 0; k < MM - 1; ++k) vload<FT, VEC>(Ub[k] + (size_t)w0[1 + k] * Ru, y0[k]);

@@ -5,7 +5,7 @@
 
 #include <atomic>
 
-#include "mttkrp_kernels.cuh"
+#include "mttkrp_planned.cuh"
 
 namespace altob {
 
@@ -22,6 +22,10 @@ altob_status launch_tiled(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
 
 template <typename FT, typename VT>
 altob_status launch_atomic_cr(const CrArgsK<FT>& a, cudaStream_t st);
+
+// Planned MTTKRP (static order 3-5, one VEC-wide chunk per lane, a.plan set).
+template <typename FT, typename VT>
+altob_status launch_planned(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps);
 
 // Batched grouped MTTKRP over the tensors of one shape class (nm = order 3-5, or 0).
 template <typename FT, typename VT>
@@ -104,6 +108,54 @@ altob_status launch_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_
     return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
 }
 
+template <typename FT, typename VT, int NM, int LPN, int V>
+altob_status launch_planned_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    static std::atomic<size_t> configured{0};
+    constexpr int mb = planned_min_blocks<FT, NM, V>();
+    if constexpr (mb > 0 && NM == 3) {
+        static std::atomic<size_t> configured_x{0};
+        const int want = env_int("ALTOB_PLAN_MINB", mb);
+        if (want != mb && (want == 2 || want == 3 || want == 4)) {
+            if (want == 2) return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 2>, configured_x, &a, c, st, bps);
+            if (want == 3) return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 3>, configured_x, &a, c, st, bps);
+            return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 4>, configured_x, &a, c, st, bps);
+        }
+    }
+    if constexpr (mb > 0)
+        return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, mb>, configured, &a, c, st, bps);
+    else
+        return launch_kernel(k_planned<FT, VT, NM, LPN, V>, configured, &a, c, st, bps);
+}
+
+template <typename FT, typename VT, int NM>
+altob_status launch_planned_shape(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    constexpr int V = 16 / sizeof(FT);
+    if (c.ch != 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned kernel shape");
+    if constexpr (sizeof(FT) == 4) {
+        if (c.vec == 8) {  // 256-bit row pieces
+            switch (c.lpn) {
+            case 1: return launch_planned_one<FT, VT, NM, 1, 8>(a, c, st, bps);
+            case 2: return launch_planned_one<FT, VT, NM, 2, 8>(a, c, st, bps);
+            case 4: return launch_planned_one<FT, VT, NM, 4, 8>(a, c, st, bps);
+            case 8: return launch_planned_one<FT, VT, NM, 8, 8>(a, c, st, bps);
+            case 16: return launch_planned_one<FT, VT, NM, 16, 8>(a, c, st, bps);
+            }
+            return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
+        }
+    }
+    if (c.vec != V) return fail(ALTOB_ERR_UNSUPPORTED, "planned kernel shape");
+    switch (c.lpn) {
+    case 2: return launch_planned_one<FT, VT, NM, 2, V>(a, c, st, bps);
+    case 4: return launch_planned_one<FT, VT, NM, 4, V>(a, c, st, bps);
+    case 8: return launch_planned_one<FT, VT, NM, 8, V>(a, c, st, bps);
+    case 16: return launch_planned_one<FT, VT, NM, 16, V>(a, c, st, bps);
+    case 32: return launch_planned_one<FT, VT, NM, 32, V>(a, c, st, bps);
+    }
+    return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
+}
+
 template <typename FT, typename VT, int NM, int LPN, int VEC, int CH>
 altob_status launch_batch_one(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
 {
@@ -165,6 +217,17 @@ altob_status launch_batch_shape(const BatchTiles<FT>& bt, const TiledCfg& c, cud
         case 5: return launch_batch_shape<FT, VT, 5>(bt, c, st, bps);                                  \
         }                                                                                              \
         return launch_batch_shape<FT, VT, 0>(bt, c, st, bps);                                          \
+    }                                                                                                  \
+    template <>                                                                                        \
+    altob_status launch_planned<FT, VT>(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st,    \
+                                        int* bps)                                                      \
+    {                                                                                                  \
+        switch (a.nmode) {                                                                             \
+        case 3: return launch_planned_shape<FT, VT, 3>(a, c, st, bps);                                 \
+        case 4: return launch_planned_shape<FT, VT, 4>(a, c, st, bps);                                 \
+        case 5: return launch_planned_shape<FT, VT, 5>(a, c, st, bps);                                 \
+        }                                                                                              \
+        return fail(ALTOB_ERR_UNSUPPORTED, "planned kernel: order 3-5");                               \
     }                                                                                                  \
     template <>                                                                                        \
     altob_status launch_atomic_cr<FT, VT>(const CrArgsK<FT>& a, cudaStream_t st)                       \

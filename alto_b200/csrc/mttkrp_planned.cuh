@@ -1,0 +1,251 @@
+// mttkrp_planned.cuh -- MTTKRP on the ALTO stream with a per-mode tile plan.
+//
+// Replaces mttkrp_alto_da_mem_pull (IntelLabs/ALTO include/alto.hpp:
+// 1227-1318) for modes with fiber reuse above 4.  The grouped kernel
+// (mttkrp_kernels.cuh) sorts every tile of the stream by output row on each
+// launch: slot claims, a scan and a counting-sort scatter, about 40% of its
+// instructions.  That order depends only on the tensor and the mode, so it is
+// computed once (k_tile_plan) and kept beside the stream as a 16-bit position
+// per nonzero and mode ("tile plan": where the nonzero goes in its tile's
+// records sorted by the mode's index, ties in stream order).  A launch then
+// reads key, value and plan entry (14 B per nonzero instead of 12), decodes
+// the mode indices and writes each record straight to its sorted slot in
+// shared memory; the run phase is the grouped kernel's (lean_runs: running
+// row sums in registers, one vector atomic per run, per-CTA hot-row
+// accumulators for long runs).  Two record buffers alternate between tiles,
+// so one barrier per tile separates the scatter from the run phase.
+//
+// The plan is the tile-local analogue of the reference's oidx (alto.hpp:
+// 246-285: a full permutation per low-reuse mode); it is built on the first
+// MTTKRP of a mode and freed with the tensor.
+#pragma once
+
+#include "mttkrp_kernels.cuh"
+
+namespace altob {
+
+typedef uint16_t u16;
+
+// Tile of the planned kernels (nonzeros per tile; plan entries are < PT_TILE).
+constexpr int PT_TILE = 1024;
+
+// Decoded high key word of the nonzeros of one tile: one value for the whole
+// tile unless it spans a run boundary of the high-word table (then two), or
+// more than two runs (then a search per nonzero).
+struct TileHi {
+    u64 hcur = 0, hnext = 0, nstart = ~0ull;
+    bool slow = false;
+    __device__ __forceinline__ void init(const KeySrc& k, u64 g0, int tile)
+    {
+        if (k.khi || k.nrun == 0) return;
+        const int r = run_of(k, g0);
+        hcur = k.run_val[r];
+        if (r + 1 < k.nrun) {
+            nstart = k.run_start[r + 1];
+            hnext = k.run_val[r + 1];
+            if (r + 2 < k.nrun && k.run_start[r + 2] < g0 + (u64)tile) slow = true;
+        }
+    }
+    __device__ __forceinline__ u64 get(const KeySrc& k, u64 g) const
+    {
+        if (k.khi) return k.khi[g];
+        if (k.nrun == 0) return 0;
+        if (slow) return key_hi(k, g);
+        return g >= nstart ? hnext : hcur;
+    }
+};
+
+// ------------------------------------------------------------ plan build
+//
+// One CTA per tile: (mode index << 32 | position in the tile) keys sorted by
+// a bitonic network in shared memory; entry g of the plan is the sorted rank
+// of nonzero g inside its tile.  Positions past the end of the stream sort
+// last and are not written.
+template <int TILE>
+__global__ void __launch_bounds__(TILE / 2) k_tile_plan(KeySrc key, Fields fld, u64 nnz, int mode, u16* plan)
+{
+    __shared__ unsigned long long s[TILE];
+    const int tid = threadIdx.x;
+    const u64 g0 = (u64)blockIdx.x * TILE;
+    const int nvalid = (int)min((u64)TILE, nnz - g0);
+    for (int i = tid; i < TILE; i += TILE / 2) {
+        unsigned long long k = ~0ull;
+        if (i < nvalid) {
+            const u64 g = g0 + i;
+            const u64 lo = key.klo[g];
+            const u64 hi = key.khi ? key.khi[g] : (key.nrun ? key_hi(key, g) : 0);
+            const u32 row = field(lo, hi, fld.pos[mode], fld.mask[mode]);
+            k = ((unsigned long long)row << 32) | (u32)i;
+        }
+        s[i] = k;
+    }
+    __syncthreads();
+    for (int k = 2; k <= TILE; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < TILE; i += TILE / 2) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long x = s[i], y = s[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        s[i] = y;
+                        s[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int p = tid; p < nvalid; p += TILE / 2) plan[g0 + (u32)s[p]] = (u16)p;
+}
+
+// --------------------------------------------------------- planned MTTKRP
+
+// Resident blocks per SM each instance is compiled for (register cap), FP32:
+// 128-bit row pieces 4 blocks of 8 warps for order 3 (as the grouped kernel)
+// and 3 for orders 4-5 (80-86 registers uncapped would allow only 2);
+// 256-bit pieces 3 for order 3 (80 registers, no spills) and 2 for orders
+// 4-5 (spills at 3).
+template <typename FT, int NM, int VEC>
+constexpr int planned_min_blocks()
+{
+    if (sizeof(FT) != 4) return 0;
+    if (VEC == 8) return NM == 3 ? 3 : 2;
+    return NM == 3 ? 4 : 3;
+}
+
+// Records a lane group takes per tile (lpn lanes per nonzero).
+constexpr int planned_ipg(int lpn) { return PT_TILE / (MT_WARPS * (32 / lpn)); }
+constexpr int log2c(int x) { return x <= 1 ? 0 : 1 + log2c(x / 2); }
+
+// Dynamic shared memory of the planned kernel: two run-ordered record
+// buffers (one padding record per lane-group stretch) and the hot-row tags.
+inline size_t planned_smem(int nmode, size_t fsz, int hot, int lpn)
+{
+    const int rw = (nmode + (int)(fsz / 4) + 3) & ~3;
+    return 2 * (size_t)(PT_TILE + PT_TILE / planned_ipg(lpn)) * rw * 4 + (size_t)hot * 4;
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC>
+__device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
+{
+    constexpr int MM = NM;
+    constexpr int RW = RecWords<FT, MM>::n;
+    constexpr int FW = (int)(sizeof(FT) / 4);
+    constexpr int NPW = 32 / LPN;
+    constexpr int NGRP = MT_WARPS * NPW;
+    constexpr int IPG = PT_TILE / NGRP;
+    constexpr int PSH = log2c(IPG);
+    constexpr int IPT = PT_TILE / MT_THREADS;
+    constexpr int SREC = PT_TILE + PT_TILE / IPG;
+    static_assert(IPG == planned_ipg(LPN) && (1 << PSH) == IPG, "lane-group stretch");
+    static_assert(NM >= 3 && NM <= ALTOB_MAX_MODES, "static order 3..5");
+    extern __shared__ __align__(16) unsigned char smem[];
+    u32* buf0 = reinterpret_cast<u32*>(smem);
+    u32* buf1 = buf0 + (size_t)SREC * RW;
+    GroupedSmem gs = {};
+    gs.htag = buf1 + (size_t)SREC * RW;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int R = a.R, target = a.target;
+    const int sub = lane % LPN, q = lane / LPN;
+    const int grp = warp * NPW + q;
+    const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
+    const VT* vals = reinterpret_cast<const VT*>(a.vals);
+    const u16* plan = a.plan;
+    if (a.hot) {
+        FT* hacc = a.hot_acc + (size_t)blockIdx.x * a.hot * R;
+        for (int k = tid; k < a.hot; k += MT_THREADS) gs.htag[k] = 0;
+        for (int k = tid; k < a.hot * R; k += MT_THREADS) hacc[k] = FT(0);
+    }
+    __syncthreads();  // the zeroed accumulators precede every run flush
+
+    int b = 0;
+    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x, b ^= 1) {
+        u32* srec = b ? buf1 : buf0;
+        const u64 g0 = ti * (u64)PT_TILE;
+        const int nvalid = (int)min((u64)PT_TILE, a.nnz - g0);
+        TileHi th;
+        th.init(a.key, g0, PT_TILE);
+        // ---- A: load key, value and plan entry; record into its sorted slot
+        u64 lo[IPT];
+        VT vv[IPT];
+        u32 ps[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int it = tid + k * MT_THREADS;
+            if (it < nvalid) {
+                const u64 g = g0 + it;
+                lo[k] = __ldcs(reinterpret_cast<const unsigned long long*>(a.key.klo) + g);
+                vv[k] = ldcs_val(vals + g);
+                ps[k] = __ldcs(reinterpret_cast<const unsigned short*>(plan) + g);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int it = tid + k * MT_THREADS;
+            if (it < nvalid) {
+                const u64 g = g0 + it;
+                const u64 hi = th.get(a.key, g);
+                u32 c[MM];
+#pragma unroll
+                for (int m = 0; m < MM; ++m) c[m] = field(lo[k], hi, a.fld.pos[m], a.fld.mask[m]);
+                u32 w[RW];
+#pragma unroll
+                for (int x = 0; x < RW; ++x) w[x] = 0u;
+                w[0] = c[0];
+#pragma unroll
+                for (int m = 1; m < MM; ++m)
+                    if (m == target) w[0] = c[m];
+#pragma unroll
+                for (int s = 1; s < MM; ++s) w[s] = s - 1 < target ? c[s - 1] : c[s];
+                const FT fv = (FT)vv[k];
+                if constexpr (FW == 1) {
+                    w[MM] = __float_as_uint((float)fv);
+                } else {
+                    const unsigned long long bits = (unsigned long long)__double_as_longlong((double)fv);
+                    w[MM] = (u32)bits;
+                    w[MM + 1] = (u32)(bits >> 32);
+                }
+                u32* dst = srec + (size_t)rslot_t<PSH>((int)ps[k]) * RW;
+#pragma unroll
+                for (int x = 0; x < RW; x += 4)
+                    *reinterpret_cast<uint4*>(dst + x) = make_uint4(w[x], w[x + 1], w[x + 2], w[x + 3]);
+            }
+        }
+        // one barrier per tile: the buffer written next tile was last read
+        // before this barrier
+        __syncthreads();
+        // ---- B: runs of equal output rows (grouped kernel's run loop)
+        gs.srec = srec;
+        const int p0 = grp * IPG;
+        const int pend = min(p0 + IPG, nvalid);
+        const FT* Uo[MM - 1];  // from the parameters each tile: fewer live registers
+#pragma unroll
+        for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : k + 1];
+        lean_runs<FT, MM, LPN, VEC, PSH>(a, gs, Uo, p0, pend, R, sub, gmask);
+    }
+    if (a.hot) {  // the CTA's hot-row sums, once each
+        const FT* hacc = a.hot_acc + (size_t)blockIdx.x * a.hot * R;
+        __syncthreads();
+        for (int k = tid; k < a.hot * R; k += MT_THREADS) {
+            const int sl = k / R;
+            const u32 tg = gs.htag[sl];
+            if (tg) atomicAdd(a.out + (size_t)(tg - 1u) * R + (k - sl * R), __ldcg(hacc + k));
+        }
+    }
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC>
+__global__ void __launch_bounds__(MT_THREADS) k_planned(TiledArgs<FT> a)
+{
+    planned_body<FT, VT, NM, LPN, VEC>(a);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int MINB>
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_planned_mb(TiledArgs<FT> a)
+{
+    planned_body<FT, VT, NM, LPN, VEC>(a);
+}
+
+}  // namespace altob

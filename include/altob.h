@@ -78,6 +78,8 @@ typedef struct {
     uint64_t device_bytes; /* HBM held by the handle */
     uint64_t key_bytes;    /* bytes of index stored per nonzero on the device */
     int nruns;             /* high index words kept as a run table (0: none) */
+    int plan_modes;        /* bit n set: mode n has a tile plan (MTTKRP) */
+    uint64_t plan_bytes;   /* HBM held by the tile plans (2 B per nonzero and mode) */
 } altob_info;
 
 /* COO tensor in host memory (SparseTensor, sptensor.hpp:8-25): cidx is
