@@ -124,6 +124,9 @@ struct AprScratch {
 
 // tt_logLikelihood (apr.hpp:851-982): lambda into mode 0, log-likelihood
 // minus sum(U_0), then mode 0 renormalised by its column 1-norms.
+// The caller provides every scratch word (lam, colacc, ll, fsum): this
+// function and the helpers it calls must not allocate device memory, since
+// altob_loglik_noalloc passes its fixed array here.
 template <typename FT>
 static altob_status loglik_impl(altob_tensor* t, FT** U, double* lam, double* colacc, double* ll, double* fsum,
                                 int R, double eps, double* out, cudaStream_t st)

@@ -80,8 +80,10 @@ def parse():
     p.add_argument("--draws", type=int, default=DRAWS, help="Zipf draws per mode (smaller = profiling case)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--cpu-sample-draws", type=int, default=40_000_000)
-    p.add_argument("--cpu-baseline-file", default=None, help=argparse.SUPPRESS)
+    p.add_argument("--cpu-baseline", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--no-serve", action="store_true", help="default workload: skip the served-stream object")
+    p.add_argument("--no-batch", action="store_true", help="default workload: skip the batched-solve object")
+    p.add_argument("--no-fp64", action="store_true", help="default workload: skip the FP64 MTTKRP companion")
     p.add_argument("--cpu-iters", type=int, default=3, help=argparse.SUPPRESS)
     p.add_argument("--workload", default="mttkrp", choices=["mttkrp", "batch", "serve", "apr", "cpals"])
     p.add_argument("--apr-nnz", type=int, default=50_000_000, help="apr: target distinct nonzeros")
@@ -164,19 +166,41 @@ def measured_peak():
 
 # --------------------------------------------------------- CPU baselines
 
-def reference_cpu_run(sample_file, iters):
-    """Runs the reference's mttkrp_alto_par sweep (oracle/_ref, or the oracle
-    port when the reference library is absent) on the sample; returns JSON."""
+def host_tensor(draws, seed):
+    """The workload's tensor in host memory: (dims, cidx (3 x nnz uint64), vals
+    float64, nnz, generator).  Generated on cuda:0 when a GPU is present (the
+    same generator and seed as the GPU arm, so both arms see the same
+    nonzeros), else by the CPU generator (same distribution, other draws)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            cidx, vals, nnz = zipf_tensor_torch(DIMS, draws, ZIPF_S, seed, "cuda")
+            hc = cidx.cpu().numpy().astype(np.uint64)
+            hv = vals.double().cpu().numpy()
+            del cidx, vals
+            torch.cuda.empty_cache()
+            return np.array(DIMS, np.uint64), hc, hv, nnz, "torch (cuda:0), as the GPU arm"
+    except ImportError:
+        pass
+    from alto_b200 import synth
+    dims, cidx, vals = synth.zipf_tensor(DIMS, draws, seed, s=ZIPF_S)
+    return dims, cidx, vals.astype(np.float64), int(vals.shape[0]), "numpy (CPU generator: other draws)"
+
+
+def ref_mttkrp_sweeps(draws, seed, iters):
+    """The reference's mttkrp_alto_par benchmark sweep (BenchmarkAlto,
+    src/main.cpp:476-495) on the workload's tensor: oracle/_ref (the
+    reference compiled from its sources) with every host thread, or the
+    oracle port when that library is absent.  Returns a dict."""
     from oracle import orc
-    d = np.load(sample_file)
-    dims, cidx, vals = d["dims"], d["cidx"], d["vals"].astype(np.float64)
-    nnz = vals.shape[0]
-    cores = os.cpu_count()
+    dims, cidx, vals, nnz, gen = host_tensor(draws, seed)
     if orc.ref_available():
         ref = orc.RefLib()
         cores = ref.max_threads()
-        t, create_s = ref.bench_mttkrp(dims, cidx, vals, cores, 128, RANK, iters, SEED)
-        kind = "reference"
+        # create_alto once (untimed by the reference itself), a warm-up
+        # sweep, then `iters` timed sweeps
+        t, create_s = ref.bench_mttkrp(dims, cidx, vals, cores, 128, RANK, iters, seed)
+        kind, march = "reference", ref.march
     else:
         o = orc.Oracle()
         at = o.create(dims, cidx, vals, 1, 128)
@@ -186,47 +210,44 @@ def reference_cpu_run(sample_file, iters):
             for m in range(3):
                 at.mttkrp(m, U, RANK)
         t = time.perf_counter() - t0
-        create_s = 0.0
-        kind, cores = "port", 1
-    value = nnz * 3 * iters / t / 1e9
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "seconds": t, "create_s": create_s,
-            "sample": f"{nnz} nonzeros ({int(d['draws'])} Zipf(1.1) draws per mode, same dims), rank {RANK}, "
-                      f"{iters} sweeps of mttkrp_alto_par over 3 modes, FP64, 128-bit ALTO index"}
-
-
-def make_cpu_sample(draws, path):
-    """Bounded sample of the workload: the same distribution with fewer
-    draws, written for the CPU process."""
-    try:
-        import torch
-        if torch.cuda.is_available():
-            cidx, vals, nnz = zipf_tensor_torch(DIMS, draws, ZIPF_S, SEED + 1000, "cuda")
-            np.savez(path, dims=np.array(DIMS, np.uint64), cidx=cidx.cpu().numpy().astype(np.uint64),
-                     vals=vals.cpu().numpy(), draws=np.int64(draws))
-            return
-    except ImportError:
-        pass
-    from alto_b200 import synth
-    dims, cidx, vals = synth.zipf_tensor(DIMS, draws, SEED + 1000, s=ZIPF_S)
-    np.savez(path, dims=dims, cidx=cidx, vals=vals.astype(np.float32), draws=np.int64(draws))
+        create_s, kind, cores, march = 0.0, "port", 1, "gcc -O2 (oracle)"
+    return {"value": nnz * 3 * iters / t / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "seconds": t,
+            "create_s": create_s, "nnz": nnz, "isa": orc.host_isa(), "build": march, "generator": gen,
+            "sample": f"the full workload ({nnz} nonzeros from {draws} Zipf(1.1) draws per mode), rank {RANK}, "
+                      f"{iters} sweeps of mttkrp_alto_par over 3 modes, FP64, 128-bit ALTO index, "
+                      f"nprtn = {cores} (OpenMP threads)"}
 
 
 def cpu_baseline(args):
-    with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "sample.npz")
-        make_cpu_sample(args.cpu_sample_draws, path)
-        env = dict(os.environ)
-        env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-        env["OMP_PROC_BIND"] = "close"
-        env["OMP_PLACES"] = "cores"
-        env["OPENBLAS_NUM_THREADS"] = "1"
-        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline-file", path, "--cpu-iters",
-                            str(args.cpu_iters)], env=env, capture_output=True, text=True, timeout=900)
-        line = [x for x in r.stdout.splitlines() if x.startswith("{")]
-        if r.returncode != 0 or not line:
-            return {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
-                    "sample": "failed: " + (r.stderr[-300:] if r.stderr else "no output")}
-        return json.loads(line[-1])
+    """The reference's sweep on the same tensor, in a child process (its
+    OpenMP settings apply there only)."""
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    env["OMP_PROC_BIND"] = "close"
+    env["OMP_PLACES"] = "cores"
+    env["OPENBLAS_NUM_THREADS"] = "1"
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-baseline", "--draws", str(args.draws),
+                        "--cpu-iters", str(args.cpu_iters)], env=env, capture_output=True, text=True, timeout=1500)
+    line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not line:
+        return {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                "sample": "failed: " + (r.stderr[-300:] if r.stderr else "no output")}
+    return json.loads(line[-1])
+
+
+def sub_workload(args, workload, extra=()):
+    """Runs `bench.py --workload <w>` in a child process (the GPU to itself)
+    and returns its JSON line, or an error record."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--workload", workload, "--steps", str(min(args.steps, 3)),
+           "--warmup", str(min(args.warmup, 3))] + list(extra)
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1200)
+    except subprocess.TimeoutExpired:
+        return {"error": "timeout"}
+    line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not line:
+        return {"error": (r.stderr[-400:] if r.stderr else "no output")}
+    return json.loads(line[-1])
 
 
 # ------------------------------------------------------------ arms
@@ -257,45 +278,25 @@ def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    from oracle import orc
-    with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "sample.npz")
-        make_cpu_sample(args.cpu_sample_draws, path)
-        d = np.load(path)
-        dims, cidx, vals = d["dims"], d["cidx"], d["vals"].astype(np.float64)
-        nnz = vals.shape[0]
-        if orc.ref_available():
-            ref = orc.RefLib()
-            cores = ref.max_threads()
-            # each call: create_alto once (untimed by the reference itself),
-            # a warm-up sweep, then `steps` timed sweeps
-            t, _ = ref.bench_mttkrp(dims, cidx, vals, cores, 128, RANK, args.steps, SEED)
-            kind = "reference"
-        else:
-            o = orc.Oracle()
-            at = o.create(dims, cidx, vals, 1, 128)
-            U = [np.random.default_rng(m).random((int(x), RANK)) for m, x in enumerate(dims)]
-            for _ in range(args.warmup):
-                for m in range(3):
-                    at.mttkrp(m, U, RANK)
-            t0 = time.perf_counter()
-            for _ in range(args.steps):
-                for m in range(3):
-                    at.mttkrp(m, U, RANK)
-            t = time.perf_counter() - t0
-            kind, cores = "port", 1
-    value = nnz * 3 * args.steps / t / 1e9
-    sample = (f"{nnz} nonzeros from {args.cpu_sample_draws} Zipf(1.1) draws per mode over the same dims; "
-              f"each step one sweep of mttkrp_alto_par over 3 modes, rank {RANK}, FP64")
+    r = ref_mttkrp_sweeps(args.draws, SEED, args.steps)
+    value = r["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "mttkrp_sweep_zipf3_4.8Mx1.8Mx1.8M", "rank": RANK, "draws": args.cpu_sample_draws,
-                       "nnz": nnz, "alto_bits": 65},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "config": workload_config(args, r["nnz"], 65, 128, ws),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "isa": r["isa"], "build": r["build"], "sample": r["sample"]},
+            "create_s": r["create_s"], "generator": r["generator"],
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(args, nnz, alto_bits, lit_bits, ws):
+    return {"workload": "mttkrp_sweep_zipf3_4.8Mx1.8Mx1.8M" if args.draws == DRAWS else
+            f"mttkrp_sweep_zipf3_small_{args.draws}", "dims": list(DIMS), "draws": args.draws, "nnz": nnz,
+            "rank": RANK, "alto_bits": alto_bits, "lit_bits": lit_bits, "parallelism": f"replicas{ws}",
+            "l2": "inputs larger than L2 (no flush)"}
 
 
 def run_altob(args):
@@ -316,7 +317,8 @@ def run_altob(args):
     cidx, vals, nnz = zipf_tensor_torch(DIMS, args.draws, ZIPF_S, rank_seed(SEED, rank), dev)
     at = ab.create_alto_device(3, np.array(DIMS, np.uint64), nnz, cidx, vals, nprtn=1024, lit_bits=128,
                                val_dtype="f32", stream=stream)
-    del cidx, vals
+    if args.no_fp64:
+        del cidx, vals
     torch.cuda.synchronize()
     info = at.info()
     g = torch.Generator(device=dev)
@@ -358,6 +360,7 @@ def run_altob(args):
         dist.barrier()
     ms = t0.elapsed_time(t1)
     clocks = clk.stop()
+    at_plan_modes = at.info()["plan_modes"]
     ms = max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
     value = ws * nnz * 3 / (ms_step / 1e3) / 1e9
@@ -416,9 +419,54 @@ def run_altob(args):
                "api": "altob_mttkrp_sweep_host (the reference's mttkrp_alto_par benchmark sweep with host "
                       "factors: copied in once, every mode, copied out)"}
 
+    # same-precision companion: FP64 values and factors, the reference's
+    # arithmetic, on the same nonzeros (device-resident, CUDA events)
+    f64 = None
+    if not args.no_fp64:
+        del out
+        at64 = ab.create_alto_device(3, np.array(DIMS, np.uint64), nnz, cidx, vals.double(), nprtn=1024,
+                                     lit_bits=128, val_dtype="f64", stream=stream)
+        del cidx, vals
+        U64 = [u.double() for u in U]
+        o64 = [torch.zeros(d, RANK, dtype=torch.float64, device=dev) for d in DIMS]
+
+        def step64():
+            for n in range(3):
+                o64[n].zero_()
+                ab.mttkrp_alto_par(n, [o64[m] if m == n else U64[m] for m in range(3)], RANK, at64, algo="auto",
+                                   accumulate=True, stream=stream)
+
+        for _ in range(3):
+            step64()
+        k64 = max(3, min(args.steps, 10))
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for _ in range(k64):
+            step64()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = f0.elapsed_time(f1) / k64
+        b64 = nnz * (info["key_bytes"] + 8) + sum(d * RANK * 8 for d in DIMS)
+        f64 = {"value": ws * nnz * 3 / (ms64 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms64, "steps": k64,
+               "dtype": "f64", "algorithmic_bytes_per_launch": b64,
+               "roofline_frac": 3 * b64 / (ms64 / 1e3) / 1e9 / peak,
+               "what": "the same sweep with FP64 values and factors (the reference's arithmetic), same nonzeros"}
+        del at64, U64, o64
+    else:
+        del out
+    del at, U
+    torch.cuda.empty_cache()
+
+    batch = serve = None
+    if rank == 0 and ws == 1 and args.draws == DRAWS:
+        if not args.no_batch:
+            batch = sub_workload(args, "batch")
+        if not args.no_serve:
+            serve = sub_workload(args, "serve")
+
     cpu = None
     if rank == 0 and not args.no_cpu and ws == 1:
-        del out
         cpu = cpu_baseline(args)
 
     if dist:
@@ -428,15 +476,13 @@ def run_altob(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "mttkrp_sweep_zipf3_4.8Mx1.8Mx1.8M" if args.draws == DRAWS else
-                           f"mttkrp_sweep_zipf3_small_{args.draws}", "dims": list(DIMS), "draws": args.draws,
-                           "nnz": nnz, "rank": RANK, "alto_bits": info["alto_bits"], "lit_bits": info["lit_bits"],
-                           "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (no flush)"},
+                "config": workload_config(args, nnz, info["alto_bits"], info["lit_bits"], ws),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                             "kernel": "k_grouped (MTTKRP)", "launch_ms_per_mode": avg_ms,
+                             "kernel": "k_planned (MTTKRP, tile plans)" if at_plan_modes == 7 else "k_grouped (MTTKRP)", "launch_ms_per_mode": avg_ms,
                              "algorithmic_bytes_per_launch": bytes_per_mode},
-                "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu}
+                "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu,
+                "fp64": f64, "batch": batch, "serve": serve}
         print(json.dumps(line), flush=True)
     return 0
 
@@ -775,8 +821,8 @@ def run_apr(args):
 
 def main():
     args = parse()
-    if args.cpu_baseline_file:
-        print(json.dumps(reference_cpu_run(args.cpu_baseline_file, args.cpu_iters)), flush=True)
+    if args.cpu_baseline:
+        print(json.dumps(ref_mttkrp_sweeps(args.draws, SEED, args.cpu_iters)), flush=True)
         return 0
     if args.impl == "reference":
         return run_reference(args)

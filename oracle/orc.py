@@ -18,6 +18,30 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_SO = os.path.join(HERE, "liborc.so")
 REF_SO = os.path.join(HERE, "_ref", "libaltoref.so")
+REF_SO_AVX512 = os.path.join(HERE, "_ref", "libaltoref_avx512.so")
+REF_SO_PEXT = os.path.join(HERE, "_ref", "libaltoref_pext.so")
+_AVX512 = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
+def host_isa():
+    """'avx512' when the host CPU has the x86-64-v4 extensions, else 'avx2'."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return "avx512" if all(x in flags for x in _AVX512) else "avx2"
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_default_path():
+    """The reference build for this host: x86-64-v4 (AVX-512) where the CPU
+    has it (the reference's own -march=native would use it), else x86-64-v3."""
+    if host_isa() == "avx512" and os.path.exists(REF_SO_AVX512):
+        return REF_SO_AVX512
+    return REF_SO
 
 _u64p = C.POINTER(C.c_uint64)
 _f64p = C.POINTER(C.c_double)
@@ -175,7 +199,10 @@ def ref_available():
 class RefLib:
     """The reference itself, compiled by oracle/build_ref.sh."""
 
-    def __init__(self, path=REF_SO):
+    def __init__(self, path=None):
+        path = path or ref_default_path()
+        self.path = path
+        self.march = "x86-64-v4" if path == REF_SO_AVX512 else "x86-64-v3"
         L = C.CDLL(path)
         L.ref_max_threads.restype = C.c_int
         L.ref_create_dump.restype = C.c_int
@@ -271,3 +298,34 @@ class RefLib:
         t = self.L.ref_bench_mttkrp(nm, _p(dims, _u64p), nnz, _p(cidx, _u64p), _p(vals, _f64p), nprtn, lit_bits,
                                     rank, iters, seed, _p(cs, _f64p))
         return t, float(cs[0])
+
+
+REF_SO_POISSON = os.path.join(HERE, "_ref", "libaltoref_poisson.so")
+
+
+class RefPoisson:
+    """The reference's own Poisson generator (PoissonGeneratorRun,
+    src/poisson_generator.cpp:337-375), compiled by oracle/build_ref.sh."""
+
+    def __init__(self, path=REF_SO_POISSON):
+        L = C.CDLL(path)
+        L.refp_run.restype = C.c_void_p
+        L.refp_run.argtypes = [C.c_int, _u64p, C.c_uint64, C.c_uint64, C.c_int, _u64p, C.c_void_p, _f64p]
+        L.refp_take.restype = None
+        L.refp_take.argtypes = [C.c_void_p, _u64p, _f64p]
+        self.L = L
+
+    def run(self, dims, num_edges, rank, nthreads):
+        """(cidx (modes x nnz), vals, U list, lambda) for `nthreads` OpenMP threads."""
+        dims = np.ascontiguousarray(dims, np.uint64)
+        nm = dims.shape[0]
+        U = [np.zeros((int(d), rank)) for d in dims]
+        lam = np.zeros(rank)
+        nnz = np.zeros(1, np.uint64)
+        h = self.L.refp_run(nm, _p(dims, _u64p), int(num_edges), int(rank), int(nthreads), _p(nnz, _u64p),
+                            _ptr_array(U), _p(lam, _f64p))
+        z = int(nnz[0])
+        cidx = np.zeros((nm, z), np.uint64)
+        vals = np.zeros(z)
+        self.L.refp_take(h, _p(cidx, _u64p), _p(vals, _f64p))
+        return cidx, vals, U, lam

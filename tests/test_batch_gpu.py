@@ -160,3 +160,34 @@ def test_batch_rejects_bad_arguments():
         b.solve(4, 0.0)
     assert e.value.status == ab.ERR_ARG
     b.close()
+
+
+def test_batch_5mode_80bit_low_reuse_vs_reference():
+    """A batch holding a 5-mode tensor with 80-bit keys (two index words) whose
+    modes all have fiber reuse <= 4 (read through oidx, op_sched), beside two
+    other tensors: each tensor's batched FP64 solve against the reference's
+    own cpd_alto (oracle/_ref) from the same seeded initial model."""
+    orc = pytest.importorskip("oracle.orc")
+    if not orc.ref_available():
+        pytest.skip("reference library oracle/_ref not built")
+    ref = orc.RefLib()
+    specs = [((50_000, 45_000, 40_000, 35_000, 60_000), 120_000, 16),
+             ((500, 400, 300), 50_000, 8),
+             ((3000, 2000, 50, 40), 40_000, 32)]
+    items, coo = [], []
+    for i, (dims, nnz, rank) in enumerate(specs):
+        d, cidx, vals = synth.uniform_distinct(dims, nnz, seed=300 + i)
+        at = ab.create_alto(ab.SparseTensor.from_arrays(d, cidx, vals), 16, 0)
+        items.append((d, at, rank))
+        coo.append((d, cidx, vals))
+    info = items[0][1].info()
+    assert info["alto_bits"] == 80 and info["lit_bits"] == 128 and info["is_oidx"]
+    iters = 6
+    fits, its, models = _batch(items, np.float64, iters, 1e-30, seeds=[21, 22, 23])
+    for k, ((d, cidx, vals), (_, at, rank)) in enumerate(zip(coo, items)):
+        rU, rlam, rfits = ref.cpd(d, cidx, vals, 16, at.info()["lit_bits"], rank, iters, 1e-30, 21 + k)
+        assert its[k] == len(rfits) == iters
+        assert np.max(np.abs(fits[k][:iters] - rfits)) < 1e-6, (k, fits[k], rfits)
+        M = models[k]
+        for n in range(len(d)):
+            assert rel_fro(M.U[n].cpu().numpy(), rU[n]) < 1e-5, (k, n)

@@ -13,37 +13,47 @@ import alto_b200 as ab
 from alto_b200 import synth
 
 pytestmark = pytest.mark.gpu
-TOL = 1e-12  # FP64 tolerance used by the parity tests
+TOL = {"f64": 1e-12, "f32": 1e-5}  # the parity tests' tolerances per model precision
 
 
-def _call(fn, at, U, lam, rank):
+def _call(fn, at, ftype, U, lam, rank, stream=None):
     ll = C.c_double(0.0)
     ptrs = (C.c_void_p * len(U))(*[u.data_ptr() for u in U])
-    st = fn(at.handle, ab.F64, ptrs, lam.data_ptr(), rank, 1e-10, C.byref(ll), None)
+    st = fn(at.handle, ftype, ptrs, lam.data_ptr(), rank, 1e-10, C.byref(ll), stream)
     assert st == 0, ab.lib().altob_last_error()
     return ll.value
 
 
-def test_loglik_noalloc_matches_loglik_on_two_calls():
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_loglik_noalloc_matches_loglik_on_two_calls(prec):
+    """Two calls in a row with different factors and lambda (the second call
+    finds the first one's values in the shared scratch); FP64 and FP32
+    models; the second pair runs on a non-default stream."""
     torch = pytest.importorskip("torch")
     dims, cidx, vals = synth.poisson_kruskal((150, 120, 90, 30), 6, 80_000, seed=12)
     at = ab.create_alto(ab.SparseTensor.from_arrays(dims, cidx, vals), 8, 0, val_dtype="u32")
     rank = 16
     L = ab.lib()
+    tol = TOL[prec]
+    dt = torch.float64 if prec == "f64" else torch.float32
+    ftype = ab.F64 if prec == "f64" else ab.F32
+    side = torch.cuda.Stream()
     for call in range(2):
         U = synth.random_factors(dims, rank, seed=40 + call)
         lam = np.linspace(0.5, 2.0, rank) * (call + 1)
-        UA = [torch.from_numpy(u.copy()).cuda() for u in U]
-        UB = [torch.from_numpy(u.copy()).cuda() for u in U]
-        lA = torch.from_numpy(lam.copy()).cuda()
-        lB = torch.from_numpy(lam.copy()).cuda()
-        want = _call(L.altob_loglik, at, UA, lA, rank)
-        got = _call(L.altob_loglik_noalloc, at, UB, lB, rank)
-        assert abs(got - want) <= TOL * abs(want), (call, got, want)
+        UA = [torch.from_numpy(u.copy()).to(dt).cuda() for u in U]
+        UB = [torch.from_numpy(u.copy()).to(dt).cuda() for u in U]
+        lA = torch.from_numpy(lam.copy()).to(dt).cuda()
+        lB = torch.from_numpy(lam.copy()).to(dt).cuda()
+        torch.cuda.synchronize()
+        stream = None if call == 0 else C.c_void_p(side.cuda_stream)
+        want = _call(L.altob_loglik, at, ftype, UA, lA, rank, stream)
+        got = _call(L.altob_loglik_noalloc, at, ftype, UB, lB, rank, stream)
+        assert abs(got - want) <= tol * abs(want), (call, got, want)
         for a, b in zip(UA, UB):
-            a, b = a.cpu().numpy(), b.cpu().numpy()
-            assert np.linalg.norm(a - b) <= TOL * np.linalg.norm(a)
-        np.testing.assert_allclose(lB.cpu().numpy(), lA.cpu().numpy(), rtol=TOL)
+            a, b = a.double().cpu().numpy(), b.double().cpu().numpy()
+            assert np.linalg.norm(a - b) <= tol * np.linalg.norm(a)
+        np.testing.assert_allclose(lB.double().cpu().numpy(), lA.double().cpu().numpy(), rtol=tol)
 
 
 def test_loglik_noalloc_rejects_rank_beyond_its_scratch():
