@@ -88,6 +88,10 @@ SIGNATURES = {
     "altob_create": (_i, [_i, _u64p, _u64, _u64p, _vp, _i, _i, _i, _vp, C.POINTER(_vp)]),
     "altob_create_device": (_i, [_i, _u64p, _u64, _vp, _vp, _i, _i, _i, _vp, C.POINTER(_vp)]),
     "altob_destroy": (_i, [_vp]),
+    "altob_slice": (_i, [_vp, _u64, _u64, _i, _vp, C.POINTER(_vp)]),
+    "altob_dump_alt_pext": (_i, [_vp, _u64p, _u64p, C.POINTER(_i), _vp]),
+    "altob_partition_ids": (_i, [_vp, _u64p, _u64p, _u64p, _vp]),
+    "altob_cpd_als_sharded": (_i, [_vp, _i, _vp, _vp, _u64, _i, _d, _dp, C.POINTER(_i), _vp, _vp, _vp]),
     "altob_get_info": (_i, [_vp, C.POINTER(_Info)]),
     "altob_dump": (_i, [_vp, _u64p, _vp, _u64p, _u64p, _u64p, _vp]),
     "altob_mttkrp": (_i, [_vp, _i, _i, _vp, _u64, _i, _i, _vp]),
@@ -106,6 +110,7 @@ SIGNATURES = {
     "altob_cpd_als_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _d, _dp, C.POINTER(_i), _vp]),
     "altob_cp_apr_host": (_i, [_vp, _i, _vp, _vp, _u64, _i, _i, _d, _d, _d, _d, _i, _dp, _vp]),
     "altob_kruskal_random_init": (_i, [_i, _u64p, _u64, C.c_uint, _i, _vp, _vp]),
+    "altob_poisson_tensor": (_i, [_i, _u64p, _u64, _u64, _i, _vp, _dp, C.POINTER(C.POINTER(_Coo)), _vp]),
     "altob_pseudo_inverse": (_i, [_vp, _i, _i, _u64, _vp, _u64, _i, C.POINTER(_i), _vp]),
     "altob_batch_create": (_i, [_vp, _i, _u64p, _i, _vp, _vp, _i, _vp, C.POINTER(_vp)]),
     "altob_batch_autotune": (_i, [_vp, _i, _vp]),
@@ -263,6 +268,36 @@ class AltoTensor:
             key_bytes=inf.key_bytes, nruns=inf.nruns, plan_modes=inf.plan_modes, plan_bytes=inf.plan_bytes,
         )
 
+    def dump_alt_pext(self, stream=None):
+        """The keys, mode masks and field positions of the reference's
+        ALT_PEXT encoding (altob_dump_alt_pext)."""
+        inf = self.info()
+        nnz, nm = inf["nnz"], inf["nmode"]
+        idx = np.zeros((nnz, 2), np.uint64)
+        masks = np.zeros((nm, 2), np.uint64)
+        pos = (C.c_int * nm)()
+        _check(lib().altob_dump_alt_pext(self.handle, idx.ctypes.data_as(_u64p), masks.ctypes.data_as(_u64p), pos,
+                                         _stream_ptr(stream)))
+        return dict(idx=idx, masks=masks, mode_pos=list(pos))
+
+    def partition_ids(self, stream=None):
+        """OPT_ALTO partition subspace ids, masks and mode masks
+        (altob_partition_ids)."""
+        inf = self.info()
+        npr, nm = inf["nprtn"], inf["nmode"]
+        pid, pmask = np.zeros(npr, np.uint64), np.zeros(npr, np.uint64)
+        mm = np.zeros((npr, nm), np.uint64)
+        _check(lib().altob_partition_ids(self.handle, pid.ctypes.data_as(_u64p), pmask.ctypes.data_as(_u64p),
+                                         mm.ctypes.data_as(_u64p), _stream_ptr(stream)))
+        return dict(prtn_id=pid, prtn_mask=pmask, prtn_mode_masks=mm)
+
+    def slice(self, begin, end, nprtn, stream=None):
+        """Nonzeros [begin, end) of the ALTO stream as a tensor of its own
+        (one GPU's share of a sharded solve; altob_slice)."""
+        h = C.c_void_p()
+        _check(lib().altob_slice(self.handle, int(begin), int(end), int(nprtn), _stream_ptr(stream), C.byref(h)))
+        return AltoTensor(h)
+
     @property
     def nmode(self):
         return self.info()["nmode"]
@@ -411,6 +446,21 @@ def KruskalModelRandomInit(M: KruskalModel, seed: int):
     ptrs = [u.ctypes.data for u in M.U]
     _check(lib().altob_kruskal_random_init(M.mode, dims.ctypes.data_as(_u64p), M.rank, int(seed) & 0xFFFFFFFF, ft,
                                            _ptr_array(ptrs), M.lam.ctypes.data))
+
+
+def poisson_tensor(dims, num_edges, rank, nthreads=1, stream=None):
+    """PoissonGeneratorRun (src/poisson_generator.cpp:337-375) as cpd64 -d
+    runs it (MakeSparseTensor, src/main.cpp:652-675), with the random streams
+    of `nthreads` OpenMP threads: (SparseTensor of counts, true model)."""
+    dims = np.ascontiguousarray(dims, np.uint64)
+    nm = dims.shape[0]
+    U = [np.zeros((int(d), int(rank))) for d in dims]
+    lam = np.zeros(int(rank))
+    p = C.POINTER(_Coo)()
+    _check(lib().altob_poisson_tensor(nm, dims.ctypes.data_as(_u64p), int(num_edges), int(rank), int(nthreads),
+                                      _ptr_array([u.ctypes.data for u in U]), lam.ctypes.data_as(_dp), C.byref(p),
+                                      _stream_ptr(stream)))
+    return _coo_to_tensor(p), KruskalModel([int(d) for d in dims], int(rank), U, lam)
 
 
 def random_init_factors(dims, rank, seed, dtype=np.float64):

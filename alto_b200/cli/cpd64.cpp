@@ -40,6 +40,8 @@ static void usage(const char* call)
     printf("Usage: %s [options]\n"
            "  -i, --input <file>     .tns text tensor\n"
            "  -b, --bin <file>       binary tensor\n"
+           "  -d, --dims <I,J,...>   generate a Poisson count tensor of these dims (rank -r)\n"
+           "  -s, --sparsity <f>     with -d: draws = f x prod(dims) (default 0.1)\n"
            "  -l, --model als|apr    decomposition\n"
            "  -r, --rank <R>         rank (default 16)\n"
            "  -m, --max-iter <N>     iterations (default 10)\n"
@@ -130,7 +132,8 @@ int main(int argc, char** argv)
     int max_iters = 10, max_inner = 10, target_mode = -1, seed = (int)time(NULL), nprtn = omp_get_max_threads();
     IType rank = 16, zero_based = 0;
     double epsilon = 1e-5;
-    std::string text_file, binary_file, model;
+    std::string text_file, binary_file, model, dims_arg;
+    double sparsity = 0.1;  // -s (main.cpp:127)
     bool do_check = false, do_bench = false;
     int c;
     while ((c = getopt_long(argc, argv, "hvi:o:b:l:r:m:n:x:d:t:s:e:f:zcp", long_opt, NULL)) != -1) {
@@ -150,10 +153,9 @@ int main(int argc, char** argv)
         case 'c': do_check = true; break;
         case 'p': do_bench = true; break;
         case 'P': nprtn = atoi(optarg); break;
-        case 'd':
-            fprintf(stderr, "-d (built-in Poisson generator) is not provided: pass -i or -b\n");
-            return -1;
-        case 'o': case 's': case 'f': break;
+        case 'd': dims_arg = optarg; break;
+        case 's': sparsity = atof(optarg); break;
+        case 'o': case 'f': break;
         default: usage(argv[0]); return -1;
         }
     }
@@ -170,8 +172,30 @@ int main(int argc, char** argv)
     try {
         if (!binary_file.empty()) ImportSparseTensor(binary_file.c_str(), BINARY_FORMAT, &X, zero_based);
         else if (!text_file.empty()) ImportSparseTensor(text_file.c_str(), TEXT_FORMAT, &X, zero_based);
-        else {
-            fprintf(stderr, "no input: use -i or -b\n");
+        else if (!dims_arg.empty()) {
+            // MakeSparseTensor (main.cpp:652-675): sparsity x prod(dims) Poisson
+            // draws from a random rank-`rank` model
+            std::vector<IType> dims;
+            size_t pos = 0;
+            while (pos <= dims_arg.size()) {
+                const size_t e = dims_arg.find(',', pos);
+                dims.push_back((IType)atoll(dims_arg.substr(pos, e == std::string::npos ? e : e - pos).c_str()));
+                if (e == std::string::npos) break;
+                pos = e + 1;
+            }
+            IType total = 1;
+            for (IType d : dims) total *= d;
+            const IType edges = (IType)(sparsity * (double)total);
+            PoissonGenerator* pg = nullptr;
+            CreatePoissonGenerator((int)dims.size(), dims.data(), &pg);
+            KruskalModel* truth = nullptr;
+            double t0 = now();
+            PoissonGeneratorRun(pg, edges, rank, &truth, &X, omp_get_max_threads());
+            printf("Creating a new tensor: %f s (%llu nonzeros)\n", now() - t0, (unsigned long long)X->nnz);
+            DestroyPoissonGenerator(pg);
+            DestroyKruskalModel(truth);
+        } else {
+            fprintf(stderr, "no input: use -i, -b or -d\n");
             return -1;
         }
         if (target_mode >= X->nmodes) {

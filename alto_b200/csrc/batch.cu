@@ -261,6 +261,32 @@ static void tune_store(const std::string& k, const TuneChoice& c)
     g_tune[k] = c;
 }
 
+// The tiles of the tensors whose target mode has a tile plan, per mode
+// (batched planned kernel; the rest of a class runs the grouped kernel).
+template <typename FT>
+struct PlannedPart {
+    int count[ALTOB_MAX_MODES] = {0};
+    TiledArgs<FT>* d_args[ALTOB_MAX_MODES] = {nullptr};
+    u64* d_prefix[ALTOB_MAX_MODES] = {nullptr};
+    int* d_bid[ALTOB_MAX_MODES] = {nullptr};
+    u64 total_tiles[ALTOB_MAX_MODES] = {0};
+    unsigned gridx = 1;
+    size_t smem = 0;
+    void free_args()
+    {
+        for (int j = 0; j < ALTOB_MAX_MODES; ++j) {
+            dfree(d_args[j]);
+            dfree(d_prefix[j]);
+            dfree(d_bid[j]);
+            d_args[j] = nullptr;
+            d_prefix[j] = nullptr;
+            d_bid[j] = nullptr;
+            total_tiles[j] = 0;
+            count[j] = 0;
+        }
+    }
+};
+
 template <typename FT>
 struct ClassRun {
     int nm = 0;  // order 3-5 (static loops), or 0 (generic)
@@ -277,6 +303,7 @@ struct ClassRun {
     u64 total_tiles[ALTOB_MAX_MODES] = {0};
     std::string key;
     float tuned_ms = -1.f;
+    PlannedPart<FT> pp;
 
     TiledCfg cfg(unsigned gx) const
     {
@@ -301,6 +328,7 @@ struct ClassRun {
             d_bid[j] = nullptr;
             total_tiles[j] = 0;
         }
+        pp.free_args();
     }
 };
 
@@ -316,6 +344,7 @@ struct LaunchGroup {
     int hmax = 0;
     unsigned gridx = 1;
     size_t smem = 0;
+    PlannedPart<FT> pp;
     int count[ALTOB_MAX_MODES] = {0};
     TiledArgs<FT>* d_args[ALTOB_MAX_MODES] = {nullptr};
     u64* d_prefix[ALTOB_MAX_MODES] = {nullptr};
@@ -345,6 +374,7 @@ struct LaunchGroup {
             d_bid[j] = nullptr;
             total_tiles[j] = 0;
         }
+        pp.free_args();
     }
 };
 
@@ -435,8 +465,9 @@ struct BatchImpl : BatchBase {
         return launch_mt(c.nm, c.vdt, bt, cfg, st, bps);
     }
 
-    // MTTKRP arguments of tensor b for target mode j with `hslots` row slots.
-    TiledArgs<FT> make_args(int b, int j, int hslots) const
+    // MTTKRP arguments of tensor b for target mode j with `hslots` row slots
+    // (and the mode's tile plan when it is read in ALTO order).
+    TiledArgs<FT> make_args(int b, int j, int hslots, bool want_plan, cudaStream_t st) const
     {
         altob_tensor* t = ts[b];
         TiledArgs<FT> a;
@@ -457,12 +488,17 @@ struct BatchImpl : BatchBase {
         for (int m = 0; m < t->nmode; ++m) a.U[m] = hdesc[b].U[m];
         a.out = hdesc[b].U[j];
         a.fld = t->fld;
+        a.plan = (want_plan && !a.perm) ? tensor_plan(t, j, st) : nullptr;
         return a;
     }
 
     // Uploads per-mode tables for (tensor, slots) members; returns counts.
-    altob_status upload_tables(const std::vector<std::pair<int, int>>& mem, TiledArgs<FT>** d_args, u64** d_prefix,
-                               int** d_bid, u64* total_tiles, int* count, cudaStream_t st)
+    // planned: 1 = the members whose mode has a tile plan, 0 = the others
+    // (a class whose kernel shape has no planned form keeps every member in
+    // the grouped tables)
+    altob_status upload_tables(const std::vector<std::pair<int, int>>& mem, int planned, bool plan_shape,
+                               TiledArgs<FT>** d_args, u64** d_prefix, int** d_bid, u64* total_tiles, int* count,
+                               cudaStream_t st)
     {
         for (int j = 0; j < maxN; ++j) {
             std::vector<TiledArgs<FT>> args;
@@ -471,7 +507,9 @@ struct BatchImpl : BatchBase {
             u64 tiles = 0;
             for (const auto& m : mem) {
                 if (ts[m.first]->nmode <= j) continue;
-                args.push_back(make_args(m.first, j, m.second));
+                TiledArgs<FT> a = make_args(m.first, j, m.second, plan_shape, st);
+                if ((a.plan != nullptr) != (planned != 0)) continue;
+                args.push_back(a);
                 prefix.push_back(tiles);
                 bid.push_back(m.first);
                 tiles += args.back().ntiles;
@@ -479,6 +517,9 @@ struct BatchImpl : BatchBase {
             prefix.push_back(tiles);
             count[j] = (int)args.size();
             total_tiles[j] = tiles;
+            d_args[j] = nullptr;
+            d_prefix[j] = nullptr;
+            d_bid[j] = nullptr;
             if (args.empty()) continue;
             ALTOB_TRY(dmalloc_t(&d_args[j], args.size()));
             ALTOB_TRY(dmalloc_t(&d_prefix[j], prefix.size()));
@@ -491,6 +532,60 @@ struct BatchImpl : BatchBase {
             ALTOB_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
         }
         return ALTOB_OK;
+    }
+
+    // Whether a kernel shape has a planned form (static order, one vector
+    // chunk per lane) and tile plans are on.
+    static bool plan_shape(int nm, int vec, int ch)
+    {
+        return nm >= 3 && ch == 1 && vec == (int)(16 / sizeof(FT)) && env_int("ALTOB_PLAN", 1);
+    }
+
+    // Tables, shared memory and grid of the planned tiles of (nm, lanes).
+    altob_status setup_planned(PlannedPart<FT>& pp, const std::vector<std::pair<int, int>>& mem, int nm,
+                               altob_dtype vdt, int lpn, int vec, int ch, cudaStream_t st)
+    {
+        pp.free_args();
+        if (!plan_shape(nm, vec, ch)) return ALTOB_OK;
+        ALTOB_TRY(upload_tables(mem, 1, true, pp.d_args, pp.d_prefix, pp.d_bid, pp.total_tiles, pp.count, st));
+        pp.smem = planned_batch_smem(nm, sizeof(FT));
+        BatchTiles<FT> bt;
+        memset(&bt, 0, sizeof(bt));
+        int bps = 0;
+        ALTOB_TRY(launch_mt(nm, vdt, bt, planned_cfg(pp, lpn, vec, ch, 0), st, &bps));
+        if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "batched planned MTTKRP kernel does not fit on an SM");
+        pp.gridx = (unsigned)(bps * num_sms());
+        return ALTOB_OK;
+    }
+
+    static TiledCfg planned_cfg(const PlannedPart<FT>& pp, int lpn, int vec, int ch, unsigned gx)
+    {
+        TiledCfg c;
+        c.lpn = lpn;
+        c.vec = vec;
+        c.ch = ch;
+        c.phi = 0;
+        c.grouped = 1;
+        c.planned = 1;
+        c.grid = dim3(gx);
+        c.smem = pp.smem;
+        return c;
+    }
+
+    altob_status mttkrp_planned(const PlannedPart<FT>& pp, int nm, altob_dtype vdt, int lpn, int vec, int ch, int j,
+                                cudaStream_t st)
+    {
+        if (!pp.d_args[j] || pp.total_tiles[j] == 0) return ALTOB_OK;
+        BatchTiles<FT> bt;
+        memset(&bt, 0, sizeof(bt));
+        bt.args = pp.d_args[j];
+        bt.tile_prefix = pp.d_prefix[j];
+        bt.bid = pp.d_bid[j];
+        bt.active = d_active;
+        bt.ntensors = pp.count[j];
+        bt.total_tiles = pp.total_tiles[j];
+        const unsigned gx = (unsigned)std::max<u64>(1, std::min<u64>(pp.total_tiles[j], pp.gridx));
+        return launch_mt(nm, vdt, bt, planned_cfg(pp, lpn, vec, ch, gx), st, nullptr);
     }
 
     // Launch groups from the classes' current choices.
@@ -519,7 +614,9 @@ struct BatchImpl : BatchBase {
                 for (int b : c->members) mem.push_back({b, c->hslots});
             }
             g->smem = grouped_smem(g->hmax, g->nm ? g->nm : ALTOB_MAX_MODES, sizeof(FT));
-            ALTOB_TRY(upload_tables(mem, g->d_args, g->d_prefix, g->d_bid, g->total_tiles, g->count, st));
+            const bool ps = plan_shape(g->nm, g->vec, g->ch);
+            ALTOB_TRY(upload_tables(mem, 0, ps, g->d_args, g->d_prefix, g->d_bid, g->total_tiles, g->count, st));
+            ALTOB_TRY(setup_planned(g->pp, mem, g->nm, g->vdt, g->lpn, g->vec, g->ch, st));
             BatchTiles<FT> bt;
             memset(&bt, 0, sizeof(bt));
             bt.hslots = g->hmax;
@@ -534,6 +631,7 @@ struct BatchImpl : BatchBase {
 
     altob_status mttkrp_group(LaunchGroup<FT>& g, int j, cudaStream_t st)
     {
+        ALTOB_TRY(mttkrp_planned(g.pp, g.nm, g.vdt, g.lpn, g.vec, g.ch, j, st));
         if (!g.d_args[j] || g.total_tiles[j] == 0) return ALTOB_OK;
         BatchTiles<FT> bt;
         bt.args = g.d_args[j];
@@ -553,7 +651,9 @@ struct BatchImpl : BatchBase {
         c.free_args();
         std::vector<std::pair<int, int>> mem;
         for (int b : c.members) mem.push_back({b, c.hslots});
-        return upload_tables(mem, c.d_args, c.d_prefix, c.d_bid, c.total_tiles, c.mode_count, st);
+        ALTOB_TRY(upload_tables(mem, 0, plan_shape(c.nm, c.vec, c.ch), c.d_args, c.d_prefix, c.d_bid,
+                                c.total_tiles, c.mode_count, st));
+        return setup_planned(c.pp, mem, c.nm, c.vdt, c.lpn, c.vec, c.ch, st);
     }
 
     // slot count and lane layout of a class -> argument tables and grid
@@ -576,6 +676,7 @@ struct BatchImpl : BatchBase {
 
     altob_status mttkrp_class(ClassRun<FT>& c, int j, cudaStream_t st)
     {
+        ALTOB_TRY(mttkrp_planned(c.pp, c.nm, c.vdt, c.lpn, c.vec, c.ch, j, st));
         if (!c.d_args[j] || c.total_tiles[j] == 0) return ALTOB_OK;
         BatchTiles<FT> bt;
         bt.args = c.d_args[j];
@@ -680,12 +781,14 @@ struct BatchImpl : BatchBase {
             int used = 0;
             for (size_t gi = 0; gi < groups.size(); ++gi) {
                 LaunchGroup<FT>& g = *groups[gi];
-                if (!g.d_args[j] || g.total_tiles[j] == 0) continue;
+                const int parts = (g.d_args[j] && g.total_tiles[j] ? 1 : 0) +
+                                  (g.pp.d_args[j] && g.pp.total_tiles[j] ? 1 : 0);
+                if (!parts) continue;
                 cudaStream_t fs = fork_st[used % NFORK];
                 if (used < NFORK) ALTOB_CUDA(cudaStreamWaitEvent(fs, fork_ev, 0));
                 ALTOB_TRY(mttkrp_group(g, j, fs));
                 ++used;
-                ++launches;
+                launches += parts;
             }
             for (int i = 0; i < std::min(used, NFORK); ++i) {
                 ALTOB_CUDA(cudaEventRecord(join_ev[i], fork_st[i]));

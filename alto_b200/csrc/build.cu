@@ -616,6 +616,14 @@ __global__ void k_gather_u64(const u64* __restrict__ src, const u64* __restrict_
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = src[idx[i]];
 }
 
+// Explicit high key word of every nonzero of a tensor that keeps them as a
+// run table.
+__global__ void k_expand_hi(KeySrc key, u64 n, u64* __restrict__ hi)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        hi[i] = key_hi(key, i);
+}
+
 static int grid_for(u64 n, int threads)
 {
     u64 blocks = (n + threads - 1) / threads;
@@ -913,6 +921,143 @@ static altob_status create_common(int nmode, const u64* dims, u64 nnz, const u64
     return ALTOB_OK;
 }
 
+// The reference's interleaved keys (default encoding, CR bits included) of
+// every nonzero, into device arrays.
+altob_status interleaved_keys(const altob_tensor* t, u64* olo, u64* ohi, cudaStream_t st)
+{
+    if (!t->nnz) return ALTOB_OK;
+    k_interleave<<<grid_for(t->nnz, 256), 256, 0, st>>>(t->d_klo, key_src(t), t->alto_bits, t->nnz, t->dec, t->fld,
+                                                        olo, ohi);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+// A contiguous range [begin, end) of a tensor's ALTO stream as a tensor of
+// its own (one GPU's share of a sharded MTTKRP or CP-ALS; the split follows
+// the reference's equal-nnz partition rule, alto.hpp:822-836).  Keys, values
+// and high words are copied; oidx (for the slice's own low-reuse modes, as
+// alto.hpp:246-285 decides them from its nonzero count), partitions and
+// intervals (alto.hpp:822-899) are computed for the slice.  The slice has no
+// CR masks: its keys keep the parent's CR bits, which no mode field reads.
+static altob_status slice_impl(const altob_tensor* t, u64 begin, u64 end, int nprtn, cudaStream_t st,
+                               altob_tensor* s)
+{
+    const u64 n = end - begin;
+    s->device = t->device;
+    s->nmode = t->nmode;
+    s->nprtn = nprtn;
+    s->lit_bits = t->lit_bits;
+    s->alto_bits = t->alto_bits;
+    s->kw = t->kw;
+    s->vdt = t->vdt;
+    s->nnz = n;
+    for (int m = 0; m < ALTOB_MAX_MODES; ++m) {
+        s->dims[m] = t->dims[m];
+        s->masks[m] = t->masks[m];
+        s->order[m] = t->order[m];
+    }
+    s->alto_mask = t->alto_mask;
+    s->dec = t->dec;
+    s->fld = t->fld;
+    const size_t vsz = val_size(t->vdt);
+    ALTOB_TRY(dmalloc_t(&s->d_klo, n));
+    ALTOB_TRY(dmalloc(&s->d_vals, n * vsz + 16));
+    if (n) {
+        ALTOB_CUDA(cudaMemcpyAsync(s->d_klo, t->d_klo + begin, n * 8, cudaMemcpyDeviceToDevice, st));
+        ALTOB_CUDA(cudaMemcpyAsync(s->d_vals, (const char*)t->d_vals + begin * vsz, n * vsz, cudaMemcpyDeviceToDevice,
+                                   st));
+    }
+    if (t->d_khi) {
+        ALTOB_TRY(dmalloc_t(&s->d_khi, n));
+        if (n) ALTOB_CUDA(cudaMemcpyAsync(s->d_khi, t->d_khi + begin, n * 8, cudaMemcpyDeviceToDevice, st));
+    } else if (t->nrun) {  // the runs that overlap the range, starts relative to it
+        std::vector<u64> rs(t->nrun), rv(t->nrun), ns, nv;
+        ALTOB_CUDA(cudaMemcpyAsync(rs.data(), t->d_run_start, rs.size() * 8, cudaMemcpyDeviceToHost, st));
+        ALTOB_CUDA(cudaMemcpyAsync(rv.data(), t->d_run_val, rv.size() * 8, cudaMemcpyDeviceToHost, st));
+        ALTOB_CUDA(cudaStreamSynchronize(st));
+        for (int r = 0; r < t->nrun; ++r) {
+            const u64 stop = r + 1 < t->nrun ? rs[r + 1] : t->nnz;
+            if (stop <= begin || rs[r] >= end) continue;
+            ns.push_back(std::max(rs[r], begin) - begin);
+            nv.push_back(rv[r]);
+        }
+        if (ns.empty()) {  // empty slice
+            ns.push_back(0);
+            nv.push_back(0);
+        }
+        ALTOB_TRY(dmalloc_t(&s->d_run_start, ns.size()));
+        ALTOB_TRY(dmalloc_t(&s->d_run_val, nv.size()));
+        ALTOB_CUDA(cudaMemcpyAsync(s->d_run_start, ns.data(), ns.size() * 8, cudaMemcpyHostToDevice, st));
+        ALTOB_CUDA(cudaMemcpyAsync(s->d_run_val, nv.data(), nv.size() * 8, cudaMemcpyHostToDevice, st));
+        s->nrun = (int)ns.size();
+    }
+    // explicit high words for the oidx and interval kernels (a run table is
+    // expanded into a temporary array)
+    const u64* hi = s->d_khi;
+    u64* hi_tmp = nullptr;
+    struct HiFree {
+        u64** p;
+        ~HiFree() { dfree(*p); }
+    } hi_free{&hi_tmp};
+    if (!hi && s->nrun && n) {
+        ALTOB_TRY(dmalloc_t(&hi_tmp, n));
+        k_expand_hi<<<grid_for(n, 256), 256, 0, st>>>(key_src(s), n, hi_tmp);
+        if (cudaGetLastError() != cudaSuccess) return fail(ALTOB_ERR_CUDA, "k_expand_hi launch failed");
+        hi = hi_tmp;
+    }
+    // oidx of the slice's low-reuse modes
+    s->is_oidx = 0;
+    for (int m = 0; m < s->nmode; ++m)
+        if (fib_reuse(s, m) <= 4) s->is_oidx = 1;
+    if (s->is_oidx && n) {
+        for (int m = 0; m < s->nmode; ++m) {
+            if (fib_reuse(s, m) > 4) continue;
+            u64 *mk = nullptr, *mk2 = nullptr;
+            u32 *io = nullptr, *io2 = nullptr;
+            altob_status a = dmalloc_t(&mk, n);
+            if (a == ALTOB_OK) a = dmalloc_t(&mk2, n);
+            if (a == ALTOB_OK) a = dmalloc_t(&io, n);
+            if (a == ALTOB_OK) a = dmalloc_t(&io2, n);
+            bool alt = false;
+            if (a == ALTOB_OK) {
+                k_mode_keys<<<grid_for(n, 256), 256, 0, st>>>(s->d_klo, hi, n, s->fld, m, mk, io);
+                if (cudaGetLastError() != cudaSuccess) a = fail(ALTOB_ERR_CUDA, "k_mode_keys launch failed");
+            }
+            if (a == ALTOB_OK) a = radix_sort_pairs(mk, nullptr, io, mk2, nullptr, io2, n, 1, mode_bits(s->dims[m]), st, &alt);
+            dfree(mk);
+            dfree(mk2);
+            if (a == ALTOB_OK) {
+                s->d_oidx[m] = alt ? io2 : io;
+                dfree(alt ? io : io2);
+            } else {
+                dfree(io);
+                dfree(io2);
+                return a;
+            }
+        }
+    }
+    // partitions and intervals of the slice
+    const int np = nprtn, nm = s->nmode;
+    const u64 per = (n + (u64)np - 1) / (u64)np;
+    s->prtn_ptr.assign(np + 1, 0);
+    for (int p = 0; p < np; ++p) s->prtn_ptr[p + 1] = std::min<u64>((u64)(p + 1) * per, n);
+    u64 dm[5] = {1, 1, 1, 1, 1};
+    for (int m = 0; m < nm; ++m) dm[m] = s->dims[m];
+    u64* d_iv = nullptr;
+    ALTOB_TRY(dmalloc_t(&d_iv, (u64)np * nm * 2));
+    k_init_intervals<<<(np * nm + 255) / 256, 256, 0, st>>>(d_iv, np, nm, dm[0], dm[1], dm[2], dm[3], dm[4]);
+    if (n) k_intervals<<<grid_for(n, 256), 256, 0, st>>>(s->d_klo, hi, n, s->fld, per, d_iv);
+    s->intervals.assign((size_t)np * nm * 2, 0);
+    cudaMemcpyAsync(s->intervals.data(), d_iv, s->intervals.size() * sizeof(u64), cudaMemcpyDeviceToHost, st);
+    const cudaError_t e = cudaStreamSynchronize(st);
+    dfree(d_iv);
+    if (e != cudaSuccess) return fail(ALTOB_ERR_CUDA, std::string("slice: ") + cudaGetErrorString(e));
+    s->device_bytes = n * (8 * (s->d_khi ? 2 : 1) + vsz) + (u64)s->nrun * 16;
+    for (int m = 0; m < nm; ++m)
+        if (s->d_oidx[m]) s->device_bytes += n * 4;
+    return ALTOB_OK;
+}
+
 }  // namespace altob
 
 using namespace altob;
@@ -973,6 +1118,27 @@ altob_status altob_create_device(int nmode, const uint64_t* dims, uint64_t nnz, 
     if (!dims) return fail(ALTOB_ERR_ARG, "dims is NULL");
     StreamScope scope((cudaStream_t)stream);
     return create_common(nmode, dims, nnz, d_cidx, d_vals, val_dtype, nprtn, lit_bits, (cudaStream_t)stream, out);
+}
+
+altob_status altob_slice(const altob_tensor* t, uint64_t begin, uint64_t end, int nprtn, void* stream,
+                         altob_tensor** out)
+{
+    if (!t || !out) return fail(ALTOB_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    if (begin > end || end > t->nnz) return fail(ALTOB_ERR_ARG, "slice range outside the tensor");
+    if (nprtn < 1) return fail(ALTOB_ERR_ARG, "nprtn must be >= 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
+    ALTOB_TRY(tensor_enter(const_cast<altob_tensor*>(t), st));
+    altob_tensor* s = new altob_tensor();
+    const altob_status r = slice_impl(t, begin, end, nprtn, st, s);
+    tensor_leave(const_cast<altob_tensor*>(t), st);
+    if (r != ALTOB_OK) {
+        altob_destroy(s);
+        return r;
+    }
+    *out = s;
+    return ALTOB_OK;
 }
 
 altob_status altob_destroy(altob_tensor* t)

@@ -24,9 +24,22 @@ struct AlsScratch {
     void* M;
 };
 
+// Cross-GPU reduction of a sharded solve (nullptr: one GPU holds the
+// whole tensor).
+struct Reducer {
+    altob_allreduce_fn fn = nullptr;
+    void* user = nullptr;
+    altob_status operator()(void* buf, u64 count, altob_dtype dt, int op, cudaStream_t st) const
+    {
+        if (!fn) return ALTOB_OK;
+        const altob_status r = fn(buf, count, dt, op, st, user);
+        return r == ALTOB_OK ? r : fail(r, "the all-reduce callback failed");
+    }
+};
+
 template <typename FT>
 static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, int max_iters, double eps,
-                                 double* fits, int* iters, cudaStream_t st)
+                                 double* fits, int* iters, cudaStream_t st, const Reducer& red = Reducer())
 {
     const int N = t->nmode;
     const u64 IN = t->dims[N - 1];
@@ -59,6 +72,7 @@ static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, in
     ALTOB_CUDA(cudaMemsetAsync(s.info, 0, sizeof(int), st));
 
     ALTOB_TRY(value_sumsq(t, s.normAT, st));
+    ALTOB_TRY(red(s.normAT, 1, ALTOB_F64, ALTOB_REDUCE_SUM, st));  // ||X||^2 over all shards
     double normAT = 0.0;
     ALTOB_CUDA(cudaMemcpyAsync(&normAT, s.normAT, sizeof(double), cudaMemcpyDeviceToHost, st));
     for (int m = 0; m < N; ++m)
@@ -72,6 +86,9 @@ static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, in
         const NormKind nk = i == 0 ? NORM_2 : NORM_MAX;
         for (int j = 0; j < N; ++j) {
             ALTOB_TRY(mttkrp_device(t, j, ft, (void* const*)U, (u64)R, 0, ALTOB_ALGO_AUTO, st));
+            // a shard's partial MTTKRP summed over the GPUs; the dense update
+            // below then runs on identical data on every GPU
+            ALTOB_TRY(red(U[j], t->dims[j] * (u64)R, ft, ALTOB_REDUCE_SUM, st));
             if (fused) {
                 double* Gj = s.G + (size_t)j * R * R;
                 double* inner = j == N - 1 ? s.inner : nullptr;
@@ -90,6 +107,9 @@ static altob_status cpd_als_impl(altob_tensor* t, FT** U, FT* lam_out, int R, in
                                j == N - 1 ? (const FT*)s.M : nullptr, s.inner, st));
         }
         ALTOB_TRY(fit_from(s.G, N, R, s.lam, s.inner, normAT, s.fit, st));
+        // one fit for every GPU (the dense passes add with atomics, so the
+        // copies may differ in the last bits): the stopping rule agrees
+        ALTOB_TRY(red(s.fit, 1, ALTOB_F64, ALTOB_REDUCE_MAX, st));
         double fit = 0.0;
         ALTOB_CUDA(cudaMemcpyAsync(&fit, s.fit, sizeof(double), cudaMemcpyDeviceToHost, st));
         ALTOB_CUDA(cudaStreamSynchronize(st));
@@ -170,4 +190,25 @@ extern "C" altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype, void* 
                                     iters, st);
     return cpd_als_impl<float>(t, (float**)d_factors, (float*)d_lambda, (int)rank, max_iters, epsilon, fits, iters,
                                st);
+}
+
+extern "C" altob_status altob_cpd_als_sharded(altob_tensor* t, altob_dtype ftype, void* const* d_factors,
+                                              void* d_lambda, uint64_t rank, int max_iters, double epsilon,
+                                              double* fits, int* iters, altob_allreduce_fn allreduce, void* user,
+                                              void* stream)
+{
+    ALTOB_TRY(check_model(t, ftype, d_factors, rank));
+    if (!allreduce) return fail(ALTOB_ERR_ARG, "allreduce callback is NULL");
+    if (max_iters < 1) return fail(ALTOB_ERR_ARG, "max_iters must be >= 1");
+    if (t->nmode < 2) return fail(ALTOB_ERR_ARG, "CP-ALS needs at least two modes");
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamScope scope(st);
+    Reducer red;
+    red.fn = allreduce;
+    red.user = user;
+    if (ftype == ALTOB_F64)
+        return cpd_als_impl<double>(t, (double**)d_factors, (double*)d_lambda, (int)rank, max_iters, epsilon, fits,
+                                    iters, st, red);
+    return cpd_als_impl<float>(t, (float**)d_factors, (float*)d_lambda, (int)rank, max_iters, epsilon, fits, iters,
+                               st, red);
 }

@@ -107,6 +107,12 @@ static bool ensure_plan(altob_tensor* t, int mode, cudaStream_t st)
     return true;
 }
 
+const uint16_t* tensor_plan(altob_tensor* t, int mode, cudaStream_t st)
+{
+    if (!env_int("ALTOB_PLAN", 1) || t->nnz == 0 || t->nnz >= (1ull << 32)) return nullptr;
+    return ensure_plan(t, mode, st) ? t->d_plan[mode] : nullptr;
+}
+
 template <typename FT, typename VT>
 static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, void* dout, u64 R, bool phi,
                                  double eps, const u32* perm, bool cache, cudaStream_t st)
@@ -150,15 +156,7 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
         a.tile = PT_TILE;
         a.ntiles = (t->nnz + PT_TILE - 1) / PT_TILE;
         a.hslots = 0;
-        // FP32 ranks that are a multiple of 8 with 32-byte aligned factors:
-        // 256-bit row pieces, R / 8 lanes per nonzero (ALTOB_VEC8=0: 128-bit)
-        bool al32 = ((uintptr_t)dout & 31u) == 0;
-        for (int m = 0; m < t->nmode; ++m) al32 = al32 && ((uintptr_t)dU[m] & 31u) == 0;
-        if (sizeof(FT) == 4 && R % 8 == 0 && R <= 128 && al32 && env_int("ALTOB_VEC8", 1)) {
-            c.vec = 8;
-            c.lpn = std::max(1, next_pow2((int)(R / 8)));
-        }
-        c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn);
+        c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn, PT_TILE, 2);
         ALTOB_TRY((launch_planned<FT, VT>(a, c, st, &bps)));
         if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned MTTKRP kernel does not fit on an SM");
         c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, (u64)bps * num_sms())));

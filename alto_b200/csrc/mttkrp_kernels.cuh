@@ -38,28 +38,15 @@ template <>
 struct VecT<double, 1> { typedef double T; };
 template <>
 struct VecT<double, 2> { typedef double2 T; };
-// 256-bit rows pieces of sm_100 (ld.global.v8.f32): 8 floats per lane
-struct __align__(32) float8_t {
-    float v[8];
-};
-template <>
-struct VecT<float, 8> { typedef float8_t T; };
 
 template <typename FT, int VEC>
 __device__ __forceinline__ void vload(const FT* p, FT* x)
 {
-    if constexpr (sizeof(FT) == 4 && VEC == 8) {  // one 256-bit load (sm_100)
-        float* f = reinterpret_cast<float*>(x);
-        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-            : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
-            : "l"(p));
-    } else {
-        typedef typename VecT<FT, VEC>::T V;
-        V v = __ldg(reinterpret_cast<const V*>(p));
-        const FT* f = reinterpret_cast<const FT*>(&v);
+    typedef typename VecT<FT, VEC>::T V;
+    V v = __ldg(reinterpret_cast<const V*>(p));
+    const FT* f = reinterpret_cast<const FT*>(&v);
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) x[e] = f[e];
-    }
+    for (int e = 0; e < VEC; ++e) x[e] = f[e];
 }
 
 template <typename FT, int VEC>
@@ -99,9 +86,6 @@ __device__ __forceinline__ void gred(FT* p, const FT* x)
 {
     if constexpr (sizeof(FT) == 4 && VEC == 4) {
         atomicAdd(reinterpret_cast<float4*>(p), make_float4(x[0], x[1], x[2], x[3]));
-    } else if constexpr (sizeof(FT) == 4 && VEC == 8) {  // no 256-bit reduction: two 128-bit ones
-        atomicAdd(reinterpret_cast<float4*>(p), make_float4(x[0], x[1], x[2], x[3]));
-        atomicAdd(reinterpret_cast<float4*>(p + 4), make_float4(x[4], x[5], x[6], x[7]));
     } else {
 #pragma unroll
         for (int e = 0; e < VEC; ++e) atomicAdd(p + e, x[e]);
@@ -1176,52 +1160,6 @@ template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI, 
 __global__ void __launch_bounds__(MT_THREADS, MINB) k_grouped_mb(TiledArgs<FT> a)
 {
     grouped_kernel_body<FT, VT, NM, LPN, VEC, CH, PHI>(a);
-}
-
-// Batched form: the tiles of many tensors (one TiledArgs each, same shape
-// class and slot count) in one persistent launch.  tile_prefix[b] is the
-// first global tile of tensor b; tensors whose active flag is 0 are skipped.
-template <typename FT>
-struct BatchTiles {
-    const TiledArgs<FT>* args;
-    const u64* tile_prefix;  // ntensors + 1
-    const int* bid;          // batch index of each entry (for `active`)
-    const int* active;
-    int ntensors;
-    int hslots;
-    u64 total_tiles;
-};
-
-template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__device__ __forceinline__ void grouped_batch_body(const BatchTiles<FT>& bt)
-{
-    constexpr int MM = grouped_mm<NM>();
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ u32 statics[2 + MT_WARPS];
-    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, bt.hslots, statics);
-    grouped_init(gs, bt.hslots);
-    for (u64 gt = blockIdx.x; gt < bt.total_tiles; gt += gridDim.x) {
-        int lo = 0, hi = bt.ntensors - 1;  // last tensor whose first tile <= gt
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (bt.tile_prefix[mid] <= gt) lo = mid;
-            else hi = mid - 1;
-        }
-        if (!bt.active[bt.bid[lo]]) continue;
-        grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(bt.args[lo], gt - bt.tile_prefix[lo], gs);
-    }
-}
-
-template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
-__global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
-{
-    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
-}
-
-template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI, int MINB>
-__global__ void __launch_bounds__(MT_THREADS, MINB) k_grouped_batch_mb(BatchTiles<FT> bt)
-{
-    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
 }
 
 template <typename FT>

@@ -13,6 +13,7 @@ struct TiledCfg {
     int lpn = 32, vec = 1, ch = 4, phi = 0;
     int grouped = 1;  // 1: k_grouped, 0: k_tiled
     int pre = 0;      // Phi from precomputed Khatri-Rao rows (grouped only)
+    int planned = 0;  // batched MTTKRP: tiles with a tile plan
     dim3 grid;
     size_t smem = 0;
 };
@@ -113,15 +114,6 @@ altob_status launch_planned_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaS
 {
     static std::atomic<size_t> configured{0};
     constexpr int mb = planned_min_blocks<FT, NM, V>();
-    if constexpr (mb > 0 && NM == 3) {
-        static std::atomic<size_t> configured_x{0};
-        const int want = env_int("ALTOB_PLAN_MINB", mb);
-        if (want != mb && (want == 2 || want == 3 || want == 4)) {
-            if (want == 2) return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 2>, configured_x, &a, c, st, bps);
-            if (want == 3) return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 3>, configured_x, &a, c, st, bps);
-            return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, 4>, configured_x, &a, c, st, bps);
-        }
-    }
     if constexpr (mb > 0)
         return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, mb>, configured, &a, c, st, bps);
     else
@@ -133,18 +125,6 @@ altob_status launch_planned_shape(const TiledArgs<FT>& a, const TiledCfg& c, cud
 {
     constexpr int V = 16 / sizeof(FT);
     if (c.ch != 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned kernel shape");
-    if constexpr (sizeof(FT) == 4) {
-        if (c.vec == 8) {  // 256-bit row pieces
-            switch (c.lpn) {
-            case 1: return launch_planned_one<FT, VT, NM, 1, 8>(a, c, st, bps);
-            case 2: return launch_planned_one<FT, VT, NM, 2, 8>(a, c, st, bps);
-            case 4: return launch_planned_one<FT, VT, NM, 4, 8>(a, c, st, bps);
-            case 8: return launch_planned_one<FT, VT, NM, 8, 8>(a, c, st, bps);
-            case 16: return launch_planned_one<FT, VT, NM, 16, 8>(a, c, st, bps);
-            }
-            return fail(ALTOB_ERR_UNSUPPORTED, "lanes per nonzero");
-        }
-    }
     if (c.vec != V) return fail(ALTOB_ERR_UNSUPPORTED, "planned kernel shape");
     switch (c.lpn) {
     case 2: return launch_planned_one<FT, VT, NM, 2, V>(a, c, st, bps);
@@ -167,10 +147,35 @@ altob_status launch_batch_one(const BatchTiles<FT>& bt, const TiledCfg& c, cudaS
         return launch_kernel(k_grouped_batch<FT, VT, NM, LPN, VEC, CH, false>, configured, &bt, c, st, bps);
 }
 
+template <typename FT, typename VT, int NM, int LPN>
+altob_status launch_planned_batch_one(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
+{
+    static std::atomic<size_t> configured{0};
+    constexpr int V = 16 / sizeof(FT);
+    constexpr int mb = planned_min_blocks<FT, NM, V>();
+    if constexpr (mb > 0)
+        return launch_kernel(k_planned_batch_mb<FT, VT, NM, LPN, V, mb>, configured, &bt, c, st, bps);
+    else
+        return launch_kernel(k_planned_batch<FT, VT, NM, LPN, V>, configured, &bt, c, st, bps);
+}
+
 template <typename FT, typename VT, int NM>
 altob_status launch_batch_shape(const BatchTiles<FT>& bt, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     constexpr int V = 16 / sizeof(FT);
+    if (c.planned) {
+        if constexpr (NM >= 3) {
+            if (c.vec != V || c.ch != 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned batch shape");
+            switch (c.lpn) {
+            case 2: return launch_planned_batch_one<FT, VT, NM, 2>(bt, c, st, bps);
+            case 4: return launch_planned_batch_one<FT, VT, NM, 4>(bt, c, st, bps);
+            case 8: return launch_planned_batch_one<FT, VT, NM, 8>(bt, c, st, bps);
+            case 16: return launch_planned_batch_one<FT, VT, NM, 16>(bt, c, st, bps);
+            case 32: return launch_planned_batch_one<FT, VT, NM, 32>(bt, c, st, bps);
+            }
+        }
+        return fail(ALTOB_ERR_UNSUPPORTED, "planned batch shape");
+    }
     if (c.vec == 1) return launch_batch_one<FT, VT, NM, 32, 1, 4>(bt, c, st, bps);
     if (c.ch == 2) {
         switch (c.lpn) {

@@ -14,6 +14,9 @@ struct TiledPlan {
 bool ptr_aligned16(const void* p);
 altob_status plan_tiled(const altob_tensor* t, u64 R, size_t fsz, bool aligned, bool cache, TiledPlan* pl);
 altob_algo resolve_algo(const altob_tensor* t, int mode, altob_algo algo);
+// The tile plan of `mode` (built on first use; nullptr when plans are off or
+// cannot be allocated).
+const uint16_t* tensor_plan(altob_tensor* t, int mode, cudaStream_t st);
 altob_status mttkrp_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, int accumulate,
                            altob_algo algo, cudaStream_t st);
 altob_status phi_device(altob_tensor* t, int mode, altob_dtype ft, void* const* dU, u64 R, double eps,

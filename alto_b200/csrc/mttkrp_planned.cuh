@@ -26,7 +26,8 @@ namespace altob {
 
 typedef uint16_t u16;
 
-// Tile of the planned kernels (nonzeros per tile; plan entries are < PT_TILE).
+// Default tile of the planned kernels (nonzeros per tile; plan entries are
+// below the tile size).
 constexpr int PT_TILE = 1024;
 
 // Decoded high key word of the nonzeros of one tile: one value for the whole
@@ -102,88 +103,60 @@ __global__ void __launch_bounds__(TILE / 2) k_tile_plan(KeySrc key, Fields fld, 
 // --------------------------------------------------------- planned MTTKRP
 
 // Resident blocks per SM each instance is compiled for (register cap), FP32:
-// 128-bit row pieces 4 blocks of 8 warps for order 3 (as the grouped kernel)
-// and 3 for orders 4-5 (80-86 registers uncapped would allow only 2);
-// 256-bit pieces 3 for order 3 (80 registers, no spills) and 2 for orders
-// 4-5 (spills at 3).
+// 4 blocks of 8 warps for order 3 (as the grouped kernel) and 3 for orders
+// 4-5 (80-86 registers uncapped would allow only 2).
 template <typename FT, int NM, int VEC>
 constexpr int planned_min_blocks()
 {
     if (sizeof(FT) != 4) return 0;
-    if (VEC == 8) return NM == 3 ? 3 : 2;
     return NM == 3 ? 4 : 3;
 }
 
 // Records a lane group takes per tile (lpn lanes per nonzero).
-constexpr int planned_ipg(int lpn) { return PT_TILE / (MT_WARPS * (32 / lpn)); }
+constexpr int planned_ipg(int pt, int lpn) { return pt / (MT_WARPS * (32 / lpn)); }
 constexpr int log2c(int x) { return x <= 1 ? 0 : 1 + log2c(x / 2); }
 
-// Dynamic shared memory of the planned kernel: two run-ordered record
+// Dynamic shared memory of the planned kernel: nbuf run-ordered record
 // buffers (one padding record per lane-group stretch) and the hot-row tags.
-inline size_t planned_smem(int nmode, size_t fsz, int hot, int lpn)
+inline size_t planned_smem(int nmode, size_t fsz, int hot, int lpn, int pt, int nbuf)
 {
     const int rw = (nmode + (int)(fsz / 4) + 3) & ~3;
-    return 2 * (size_t)(PT_TILE + PT_TILE / planned_ipg(lpn)) * rw * 4 + (size_t)hot * 4;
+    return (size_t)nbuf * (size_t)(pt + pt / planned_ipg(pt, lpn)) * rw * 4 + (size_t)hot * 4;
 }
 
-template <typename FT, typename VT, int NM, int LPN, int VEC>
-__device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
+// Phase A of a planned tile: every thread loads key, value and plan entry
+// of its nonzeros (four in flight at a time), decodes the mode indices and
+// writes the record [target, other modes..., value] to its run-ordered slot
+// (one padding record per 2^PSH).
+template <typename FT, typename VT, int MM, int PT, int PSH>
+__device__ __forceinline__ void planned_scatter(const TiledArgs<FT>& a, u64 g0, int nvalid, u32* srec)
 {
-    constexpr int MM = NM;
     constexpr int RW = RecWords<FT, MM>::n;
     constexpr int FW = (int)(sizeof(FT) / 4);
-    constexpr int NPW = 32 / LPN;
-    constexpr int NGRP = MT_WARPS * NPW;
-    constexpr int IPG = PT_TILE / NGRP;
-    constexpr int PSH = log2c(IPG);
-    constexpr int IPT = PT_TILE / MT_THREADS;
-    constexpr int SREC = PT_TILE + PT_TILE / IPG;
-    static_assert(IPG == planned_ipg(LPN) && (1 << PSH) == IPG, "lane-group stretch");
-    static_assert(NM >= 3 && NM <= ALTOB_MAX_MODES, "static order 3..5");
-    extern __shared__ __align__(16) unsigned char smem[];
-    u32* buf0 = reinterpret_cast<u32*>(smem);
-    u32* buf1 = buf0 + (size_t)SREC * RW;
-    GroupedSmem gs = {};
-    gs.htag = buf1 + (size_t)SREC * RW;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int R = a.R, target = a.target;
-    const int sub = lane % LPN, q = lane / LPN;
-    const int grp = warp * NPW + q;
-    const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
+    constexpr int IPT = PT / MT_THREADS;
+    constexpr int IPQ = IPT < 4 ? IPT : 4;
+    const int tid = threadIdx.x, target = a.target;
     const VT* vals = reinterpret_cast<const VT*>(a.vals);
-    const u16* plan = a.plan;
-    if (a.hot) {
-        FT* hacc = a.hot_acc + (size_t)blockIdx.x * a.hot * R;
-        for (int k = tid; k < a.hot; k += MT_THREADS) gs.htag[k] = 0;
-        for (int k = tid; k < a.hot * R; k += MT_THREADS) hacc[k] = FT(0);
-    }
-    __syncthreads();  // the zeroed accumulators precede every run flush
-
-    int b = 0;
-    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x, b ^= 1) {
-        u32* srec = b ? buf1 : buf0;
-        const u64 g0 = ti * (u64)PT_TILE;
-        const int nvalid = (int)min((u64)PT_TILE, a.nnz - g0);
-        TileHi th;
-        th.init(a.key, g0, PT_TILE);
-        // ---- A: load key, value and plan entry; record into its sorted slot
-        u64 lo[IPT];
-        VT vv[IPT];
-        u32 ps[IPT];
+    TileHi th;
+    th.init(a.key, g0, PT);
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int it = tid + k * MT_THREADS;
+    for (int k0 = 0; k0 < IPT; k0 += IPQ) {
+        u64 lo[IPQ];
+        VT vv[IPQ];
+        u32 ps[IPQ];
+#pragma unroll
+        for (int k = 0; k < IPQ; ++k) {
+            const int it = tid + (k0 + k) * MT_THREADS;
             if (it < nvalid) {
                 const u64 g = g0 + it;
                 lo[k] = __ldcs(reinterpret_cast<const unsigned long long*>(a.key.klo) + g);
                 vv[k] = ldcs_val(vals + g);
-                ps[k] = __ldcs(reinterpret_cast<const unsigned short*>(plan) + g);
+                ps[k] = __ldcs(reinterpret_cast<const unsigned short*>(a.plan) + g);
             }
         }
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int it = tid + k * MT_THREADS;
+        for (int k = 0; k < IPQ; ++k) {
+            const int it = tid + (k0 + k) * MT_THREADS;
             if (it < nvalid) {
                 const u64 g = g0 + it;
                 const u64 hi = th.get(a.key, g);
@@ -213,8 +186,79 @@ __device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
                     *reinterpret_cast<uint4*>(dst + x) = make_uint4(w[x], w[x + 1], w[x + 2], w[x + 3]);
             }
         }
-        // one barrier per tile: the buffer written next tile was last read
-        // before this barrier
+    }
+}
+
+// One planned tile with one record buffer (the batched kernel): scatter,
+// barrier, runs, barrier.  The records use the grouped kernel's padding (one
+// per 32), so the buffer is the grouped kernel's run-ordered record area.
+template <typename FT, typename VT, int NM, int LPN, int VEC>
+__device__ __forceinline__ void planned_tile(const TiledArgs<FT>& a, u64 ti, const GroupedSmem& gs)
+{
+    constexpr int NPW = 32 / LPN;
+    constexpr int IPG = PT_TILE / (MT_WARPS * NPW);
+    static_assert(NM >= 3 && NM <= ALTOB_MAX_MODES, "static order 3..5");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int sub = lane % LPN, q = lane / LPN;
+    const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
+    const u64 g0 = ti * (u64)PT_TILE;
+    const int nvalid = (int)min((u64)PT_TILE, a.nnz - g0);
+    planned_scatter<FT, VT, NM, PT_TILE, 5>(a, g0, nvalid, gs.srec);
+    __syncthreads();
+    const int p0 = (warp * NPW + q) * IPG;
+    const FT* Uo[NM - 1];
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) Uo[k] = a.U[k < a.target ? k : k + 1];
+    lean_runs<FT, NM, LPN, VEC, 5>(a, gs, Uo, p0, min(p0 + IPG, nvalid), a.R, sub, gmask);
+    __syncthreads();
+}
+
+// PT: nonzeros per tile (the plan's tile); NBUF: record buffers (2: the
+// next tile's scatter overlaps this tile's runs, one barrier per tile; 1:
+// two barriers per tile, half the shared memory, so more of the SM's
+// 256 KB stays L1 cache for the row gathers).
+template <typename FT, typename VT, int NM, int LPN, int VEC, int PT, int NBUF>
+__device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
+{
+    constexpr int MM = NM;
+    constexpr int RW = RecWords<FT, MM>::n;
+    constexpr int NPW = 32 / LPN;
+    constexpr int NGRP = MT_WARPS * NPW;
+    constexpr int IPG = PT / NGRP;
+    constexpr int PSH = log2c(IPG);
+    constexpr int SREC = PT + PT / IPG;
+    static_assert(IPG == planned_ipg(PT, LPN) && (1 << PSH) == IPG, "lane-group stretch");
+    static_assert(NM >= 3 && NM <= ALTOB_MAX_MODES, "static order 3..5");
+    static_assert(NBUF == 1 || NBUF == 2, "record buffers");
+    extern __shared__ __align__(16) unsigned char smem[];
+    u32* buf0 = reinterpret_cast<u32*>(smem);
+    u32* buf1 = buf0 + (NBUF - 1) * (size_t)SREC * RW;
+    GroupedSmem gs = {};
+    gs.htag = buf1 + (size_t)SREC * RW;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int R = a.R, target = a.target;
+    const int sub = lane % LPN, q = lane / LPN;
+    const int grp = warp * NPW + q;
+    const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
+    if (a.hot) {
+        FT* hacc = a.hot_acc + (size_t)blockIdx.x * a.hot * R;
+        for (int k = tid; k < a.hot; k += MT_THREADS) gs.htag[k] = 0;
+        for (int k = tid; k < a.hot * R; k += MT_THREADS) hacc[k] = FT(0);
+    }
+    __syncthreads();  // the zeroed accumulators precede every run flush
+
+    int b = 0;
+    for (u64 ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x, b ^= 1) {
+        u32* srec = b ? buf1 : buf0;
+        const u64 g0 = ti * (u64)PT;
+        const int nvalid = (int)min((u64)PT, a.nnz - g0);
+        TileHi th;
+        th.init(a.key, g0, PT);
+        // ---- A: load key, value and plan entry; record into its sorted slot
+        planned_scatter<FT, VT, MM, PT, PSH>(a, g0, nvalid, srec);
+        // with two buffers one barrier per tile: the buffer written next tile
+        // was last read before this barrier
         __syncthreads();
         // ---- B: runs of equal output rows (grouped kernel's run loop)
         gs.srec = srec;
@@ -224,6 +268,7 @@ __device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
 #pragma unroll
         for (int k = 0; k < MM - 1; ++k) Uo[k] = a.U[k < target ? k : k + 1];
         lean_runs<FT, MM, LPN, VEC, PSH>(a, gs, Uo, p0, pend, R, sub, gmask);
+        if constexpr (NBUF == 1) __syncthreads();  // the records are overwritten next tile
     }
     if (a.hot) {  // the CTA's hot-row sums, once each
         const FT* hacc = a.hot_acc + (size_t)blockIdx.x * a.hot * R;
@@ -236,16 +281,101 @@ __device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
     }
 }
 
-template <typename FT, typename VT, int NM, int LPN, int VEC>
+template <typename FT, typename VT, int NM, int LPN, int VEC, int PT = PT_TILE, int NBUF = 2>
 __global__ void __launch_bounds__(MT_THREADS) k_planned(TiledArgs<FT> a)
 {
-    planned_body<FT, VT, NM, LPN, VEC>(a);
+    planned_body<FT, VT, NM, LPN, VEC, PT, NBUF>(a);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int MINB, int PT = PT_TILE, int NBUF = 2>
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_planned_mb(TiledArgs<FT> a)
+{
+    planned_body<FT, VT, NM, LPN, VEC, PT, NBUF>(a);
+}
+
+// Batched form: the tiles of many tensors (one TiledArgs each, same shape
+// class and slot count) in one persistent launch.  tile_prefix[b] is the
+// first global tile of tensor b; tensors whose active flag is 0 are skipped.
+template <typename FT>
+struct BatchTiles {
+    const TiledArgs<FT>* args;
+    const u64* tile_prefix;  // ntensors + 1
+    const int* bid;          // batch index of each entry (for `active`)
+    const int* active;
+    int ntensors;
+    int hslots;
+    u64 total_tiles;
+};
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__device__ __forceinline__ void grouped_batch_body(const BatchTiles<FT>& bt)
+{
+    constexpr int MM = grouped_mm<NM>();
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 statics[2 + MT_WARPS];
+    const GroupedSmem gs = grouped_smem_ptrs<FT, MM>(smem, bt.hslots, statics);
+    grouped_init(gs, bt.hslots);
+    for (u64 gt = blockIdx.x; gt < bt.total_tiles; gt += gridDim.x) {
+        int lo = 0, hi = bt.ntensors - 1;  // last tensor whose first tile <= gt
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bt.tile_prefix[mid] <= gt) lo = mid;
+            else hi = mid - 1;
+        }
+        if (!bt.active[bt.bid[lo]]) continue;
+        grouped_tile<FT, VT, NM, LPN, VEC, CH, PHI>(bt.args[lo], gt - bt.tile_prefix[lo], gs);
+    }
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI>
+__global__ void __launch_bounds__(MT_THREADS) k_grouped_batch(BatchTiles<FT> bt)
+{
+    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC, int CH, bool PHI, int MINB>
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_grouped_batch_mb(BatchTiles<FT> bt)
+{
+    grouped_batch_body<FT, VT, NM, LPN, VEC, CH, PHI>(bt);
+}
+
+// Batched planned MTTKRP: the tiles of the tensors whose target mode has a
+// tile plan (same shape class), one persistent launch; single record buffer.
+template <typename FT, typename VT, int NM, int LPN, int VEC>
+__device__ __forceinline__ void planned_batch_body(const BatchTiles<FT>& bt)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    GroupedSmem gs = {};
+    gs.srec = reinterpret_cast<u32*>(smem);
+    for (u64 gt = blockIdx.x; gt < bt.total_tiles; gt += gridDim.x) {
+        int lo = 0, hi = bt.ntensors - 1;  // last tensor whose first tile <= gt
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bt.tile_prefix[mid] <= gt) lo = mid;
+            else hi = mid - 1;
+        }
+        if (!bt.active[bt.bid[lo]]) continue;
+        planned_tile<FT, VT, NM, LPN, VEC>(bt.args[lo], gt - bt.tile_prefix[lo], gs);
+    }
+}
+
+template <typename FT, typename VT, int NM, int LPN, int VEC>
+__global__ void __launch_bounds__(MT_THREADS) k_planned_batch(BatchTiles<FT> bt)
+{
+    planned_batch_body<FT, VT, NM, LPN, VEC>(bt);
 }
 
 template <typename FT, typename VT, int NM, int LPN, int VEC, int MINB>
-__global__ void __launch_bounds__(MT_THREADS, MINB) k_planned_mb(TiledArgs<FT> a)
+__global__ void __launch_bounds__(MT_THREADS, MINB) k_planned_batch_mb(BatchTiles<FT> bt)
 {
-    planned_body<FT, VT, NM, LPN, VEC>(a);
+    planned_batch_body<FT, VT, NM, LPN, VEC>(bt);
+}
+
+// Shared memory of the batched planned kernel: one run-ordered record buffer.
+inline size_t planned_batch_smem(int nmode, size_t fsz)
+{
+    const int rw = (nmode + (int)(fsz / 4) + 3) & ~3;
+    return (size_t)(PT_TILE + PT_TILE / 32) * rw * 4;
 }
 
 }  // namespace altob

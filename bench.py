@@ -320,6 +320,7 @@ def run_altob(args):
     if args.no_fp64:
         del cidx, vals
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # the generator's temporaries: a profiler saves every allocation
     info = at.info()
     g = torch.Generator(device=dev)
     g.manual_seed(SEED)

@@ -121,6 +121,36 @@ inline void ExportSparseTensor(const char* file_path, FileFormat f, SparseTensor
     altob_detail::check(s, "ExportSparseTensor");
 }
 
+// ------------------------------------------------- Poisson generator
+// PoissonGenerator / PoissonGeneratorRun (src/poisson_generator.cpp:
+// 99-375) on top of altob_poisson_tensor: the random streams of the
+// caller's OpenMP thread count, the edges drawn and merged on the device.
+struct PoissonGenerator {
+    int mode;
+    IType* dims;
+};
+
+inline void CreatePoissonGenerator(int mode, IType* dims, PoissonGenerator** pg_)
+{
+    PoissonGenerator* pg = (PoissonGenerator*)calloc(1, sizeof(PoissonGenerator));
+    pg->mode = mode;
+    pg->dims = (IType*)malloc(sizeof(IType) * mode);
+    memcpy(pg->dims, dims, sizeof(IType) * mode);
+    *pg_ = pg;
+}
+
+inline void DestroyPoissonGenerator(PoissonGenerator* pg)
+{
+    if (!pg) return;
+    free(pg->dims);
+    free(pg);
+}
+
+struct KruskalModel;
+inline void CreateKruskalModel(int mode, IType* dims, IType rank, KruskalModel** M_);
+inline void PoissonGeneratorRun(PoissonGenerator* pg, IType num_edges, IType rank, KruskalModel** M_,
+                                SparseTensor** X_, int nthreads);
+
 // ------------------------------------------------------- Kruskal model
 struct KruskalModel {
     int mode;
@@ -141,6 +171,46 @@ inline void CreateKruskalModel(int mode, IType* dims, IType rank, KruskalModel**
     for (int n = 0; n < mode; ++n) M->U[n] = (FType*)malloc(sizeof(FType) * dims[n] * rank);
     M->lambda = (FType*)malloc(sizeof(FType) * rank);
     *M_ = M;
+}
+
+// nthreads: the OpenMP thread count whose random streams are replayed (the
+// reference uses omp_get_max_threads()).
+inline void PoissonGeneratorRun(PoissonGenerator* pg, IType num_edges, IType rank, KruskalModel** M_,
+                                SparseTensor** X_, int nthreads)
+{
+    const int N = pg->mode;
+    std::vector<std::vector<double>> U(N);
+    std::vector<double*> up(N);
+    for (int n = 0; n < N; ++n) {
+        U[n].resize(pg->dims[n] * rank);
+        up[n] = U[n].data();
+    }
+    std::vector<double> lam(rank);
+    std::vector<uint64_t> d(pg->dims, pg->dims + N);
+    altob_coo* c = nullptr;
+    altob_detail::check(altob_poisson_tensor(N, d.data(), num_edges, rank, nthreads, up.data(), lam.data(), &c, nullptr),
+                        "PoissonGeneratorRun");
+    KruskalModel* M = nullptr;
+    CreateKruskalModel(N, pg->dims, rank, &M);
+    for (int n = 0; n < N; ++n)
+        for (IType i = 0; i < pg->dims[n] * rank; ++i) M->U[n][i] = (FType)U[n][i];
+    for (IType r = 0; r < rank; ++r) M->lambda[r] = (FType)lam[r];
+    SparseTensor* X = (SparseTensor*)calloc(1, sizeof(SparseTensor));
+    X->nmodes = c->nmode;
+    X->nnz = c->nnz;
+    X->dims = (IType*)malloc(sizeof(IType) * c->nmode);
+    X->cidx = (IType**)malloc(sizeof(IType*) * c->nmode);
+    IType* block = (IType*)malloc(sizeof(IType) * c->nmode * (c->nnz ? c->nnz : 1));
+    memcpy(block, c->cidx, sizeof(IType) * c->nmode * c->nnz);
+    for (int n = 0; n < c->nmode; ++n) {
+        X->dims[n] = c->dims[n];
+        X->cidx[n] = block + (size_t)n * c->nnz;
+    }
+    X->vals = (FType*)malloc(sizeof(FType) * (c->nnz ? c->nnz : 1));
+    for (IType i = 0; i < c->nnz; ++i) X->vals[i] = (FType)c->vals[i];
+    altob_coo_free(c);
+    *M_ = M;
+    *X_ = X;
 }
 
 inline void KruskalModelRandomInit(KruskalModel* M, unsigned int seed)

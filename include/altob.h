@@ -120,6 +120,16 @@ ALTOB_API altob_status altob_create_device(int nmode, const uint64_t* dims, uint
 /* Replaces destroy_alto (alto.hpp:296-322). */
 ALTOB_API altob_status altob_destroy(altob_tensor* t);
 
+/* One GPU's share of a sharded MTTKRP / CP-ALS: nonzeros [begin, end) of
+ * t's ALTO stream (the reference's contiguous equal-nnz partitions,
+ * prtn_alto, alto.hpp:822-836, with one partition per GPU) as a tensor of
+ * its own with nprtn partitions, mode intervals (alto.hpp:874-899) and oidx
+ * (alto.hpp:246-285) computed for the slice; t is unchanged and may be
+ * destroyed afterwards.  The slice has no conflict-resolution masks. */
+ALTOB_API altob_status altob_slice(const altob_tensor* t, uint64_t begin,
+                                   uint64_t end, int nprtn, void* stream,
+                                   altob_tensor** out);
+
 ALTOB_API altob_status altob_get_info(const altob_tensor* t, altob_info* out);
 
 /* Copies the encoding back to the host in the reference's layout (for
@@ -130,6 +140,26 @@ ALTOB_API altob_status altob_get_info(const altob_tensor* t, altob_info* out);
 ALTOB_API altob_status altob_dump(const altob_tensor* t, uint64_t* idx, void* vals,
                         uint64_t* prtn_ptr, uint64_t* intervals,
                         uint64_t* oidx, void* stream);
+
+/* The keys and mode masks a -DALT_PEXT build of the reference holds
+ * (alto.hpp:212-244): every mode index re-encoded as a bit field at
+ * mode_pos[n] (the running sum of bit counts in mode order, alto.hpp:
+ * 695-700), CR bits kept; masks (1 << bits) - 1.  idx: nnz (lo, hi) pairs;
+ * mode_masks: nmode (lo, hi) pairs; mode_pos: nmode; any may be NULL.  Modes
+ * of 31 or more bits are refused (the reference's int mask expression is
+ * undefined there). */
+ALTOB_API altob_status altob_dump_alt_pext(const altob_tensor* t, uint64_t* idx,
+                                           uint64_t* mode_masks, int* mode_pos,
+                                           void* stream);
+
+/* The partition subspace ids of a -DOPT_ALTO build (alto.hpp:838-868), per
+ * partition p: the ALTO bits its first and last keys share (before CR bits),
+ * prtn_id[p] = those bits, prtn_mask[p] = their mask, prtn_mode_masks[p *
+ * nmode + n] = mode n's mask restricted to them; 64-bit words as in the
+ * reference; empty partitions 0. */
+ALTOB_API altob_status altob_partition_ids(const altob_tensor* t, uint64_t* prtn_id,
+                                           uint64_t* prtn_mask,
+                                           uint64_t* prtn_mode_masks, void* stream);
 
 /* ---- MTTKRP ------------------------------------------------------------
  * Replaces mttkrp_alto_par(int target_mode, FType** factors, IType rank,
@@ -164,6 +194,29 @@ ALTOB_API altob_status altob_cpd_als(altob_tensor* t, altob_dtype ftype,
                            void* const* d_factors, void* d_lambda,
                            uint64_t rank, int max_iters, double epsilon,
                            double* fits, int* iters, void* stream);
+
+/* Sharded CP-ALS (no counterpart in the reference, which runs on one
+ * node): every GPU holds one slice of the tensor (altob_slice) and the whole
+ * model, and runs cpd_alto (cpd.hpp:43-186) with three exchanges, made by the
+ * caller's allreduce callback (for example an NCCL all-reduce on `stream`):
+ * the norm of the tensor once (sum), each mode's partial MTTKRP (sum over
+ * the GPUs, dims[mode] x rank values of ftype, in place) and each
+ * iteration's fit (max, so every GPU takes the same stopping decision).  The
+ * dense update then runs on identical data on every GPU.  Every GPU must call
+ * this with the same model, rank, max_iters and epsilon; the callback must
+ * return ALTOB_OK after the reduction, or an error status, which ends the
+ * solve on that GPU (the others then fail in their next exchange). */
+#define ALTOB_REDUCE_SUM 0
+#define ALTOB_REDUCE_MAX 1
+typedef altob_status (*altob_allreduce_fn)(void* d_buf, uint64_t count,
+                                           altob_dtype dtype, int op,
+                                           void* stream, void* user);
+ALTOB_API altob_status altob_cpd_als_sharded(altob_tensor* slice, altob_dtype ftype,
+                                             void* const* d_factors, void* d_lambda,
+                                             uint64_t rank, int max_iters, double epsilon,
+                                             double* fits, int* iters,
+                                             altob_allreduce_fn allreduce, void* user,
+                                             void* stream);
 
 /* Replaces pseudo_inverse (cpd.hpp:546-646): U <- U V^-1 with V the
  * Hadamard product of the Grams of every mode but `mode` (d_grams: nmode
@@ -345,6 +398,26 @@ ALTOB_API altob_status altob_server_stats(const altob_server* s, uint64_t* used_
                                           uint64_t* peak_bytes, int* queued, int* running);
 /* Finishes the queued requests, then stops the workers. */
 ALTOB_API altob_status altob_server_destroy(altob_server* s);
+
+/* Replaces PoissonGeneratorRun (src/poisson_generator.cpp:337-375) as
+ * MakeSparseTensor (src/main.cpp:652-675, cpd64 -d) calls it: a random
+ * rank-`rank` Kruskal model (GenerateRandomModel :145-194), num_edges
+ * multinomial draws of its components and coordinates (GenerateEdges
+ * :197-259), duplicates merged into counts (ConstructCIdx :262-334).  The
+ * reference's random streams (one MT19937-64 per OpenMP thread, seeded
+ * 1234 + thread id, and the C library's rand() from its initial state) are
+ * replayed for `nthreads` threads; the edges are drawn and sorted on the
+ * device.  For the same thread count the tensor and the model equal the
+ * reference's (above one thread up to the order in which the reference's
+ * OpenMP reduction adds its column sums).  *out: host COO (0-based,
+ * values = counts), freed with altob_coo_free; model_U (nmode host arrays,
+ * dims[n] x rank, FP64) and model_lambda (rank) receive the model and may
+ * be NULL.  Every dimension must be >= rank (the reference asserts it). */
+ALTOB_API altob_status altob_poisson_tensor(int nmode, const uint64_t* dims,
+                                            uint64_t num_edges, uint64_t rank,
+                                            int nthreads, double* const* model_U,
+                                            double* model_lambda, altob_coo** out,
+                                            void* stream);
 
 /* ---- tensor files ------------------------------------------------------
  * Replaces ImportSparseTensor (sptensor.cpp:165-258).  The .tns reader

@@ -54,6 +54,9 @@ p2=$!
 # mode's bits contiguous
 build x86-64-v3 libaltoref_pext.so -DALT_PEXT &
 p3=$!
+# the OPT_ALTO build (alto.hpp:838-868): partition subspace ids
+build x86-64-v3 libaltoref_opt.so -DOPT_ALTO &
+p5=$!
 # the reference's Poisson generator (src/poisson_generator.cpp, rng.cpp,
 # rng_stream.cpp) for the generator's parity tests; floating-point
 # contraction off so that uniform(low, high) = x * (high - low) + low rounds
@@ -71,4 +74,5 @@ wait $p1
 wait $p2
 wait $p3
 wait $p4
+wait $p5
 echo "built $OUT/libaltoref_poisson.so (-ffp-contract=off)"

@@ -20,6 +20,7 @@ ORC_SO = os.path.join(HERE, "liborc.so")
 REF_SO = os.path.join(HERE, "_ref", "libaltoref.so")
 REF_SO_AVX512 = os.path.join(HERE, "_ref", "libaltoref_avx512.so")
 REF_SO_PEXT = os.path.join(HERE, "_ref", "libaltoref_pext.so")
+REF_SO_OPT = os.path.join(HERE, "_ref", "libaltoref_opt.so")
 _AVX512 = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
 
 
@@ -291,6 +292,20 @@ class RefLib:
         L.ref_write.argtypes = [C.c_char_p, C.c_int, C.c_int, _u64p, C.c_uint64, _u64p, _f64p]
         dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)
         L.ref_write(path.encode(), int(bool(binary)), nm, _p(dims, _u64p), nnz, _p(cidx, _u64p), _p(vals, _f64p))
+
+    def prtn_ids(self, dims, cidx, vals, nprtn, lit_bits):
+        """OPT_ALTO partition ids (a -DOPT_ALTO build only)."""
+        dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)
+        L = self.L
+        L.ref_prtn_ids.restype = C.c_int
+        L.ref_prtn_ids.argtypes = [C.c_int, _u64p, C.c_uint64, _u64p, _f64p, C.c_int, C.c_int, _u64p, _u64p, _u64p]
+        pid, pm = np.zeros(nprtn, np.uint64), np.zeros(nprtn, np.uint64)
+        mm = np.zeros((nprtn, nm), np.uint64)
+        rc = L.ref_prtn_ids(nm, _p(dims, _u64p), nnz, _p(cidx, _u64p), _p(vals, _f64p), nprtn, lit_bits,
+                            _p(pid, _u64p), _p(pm, _u64p), _p(mm, _u64p))
+        if rc != 0:
+            raise RuntimeError("this reference build has no OPT_ALTO")
+        return dict(prtn_id=pid, prtn_mask=pm, prtn_mode_masks=mm)
 
     def bench_mttkrp(self, dims, cidx, vals, nprtn, lit_bits, rank, iters, seed):
         dims, cidx, vals, nm, nnz = _coo_args(dims, cidx, vals)

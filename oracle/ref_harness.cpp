@@ -22,6 +22,7 @@
 #include "apr.hpp"
 
 #include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -334,6 +335,35 @@ double ref_bench_mttkrp(int nmode, const uint64_t* dims, uint64_t nnz,
         : run_bench<unsigned long long>(X, nprtn, rank, iters, seed, create_s);
     DestroySparseTensor(X);
     return t;
+}
+
+// OPT_ALTO partition subspace ids (alto.hpp:838-868) of the encoding
+// create_alto builds; -1 in builds without OPT_ALTO.
+int ref_prtn_ids(int nmode, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx, const double* vals, int nprtn,
+                 int lit_bits, uint64_t* prtn_id, uint64_t* prtn_mask, uint64_t* prtn_mode_masks)
+{
+#ifdef OPT_ALTO
+    SparseTensor* X = make_spt(nmode, dims, nnz, cidx, vals);
+    auto run = [&](auto* tag) {
+        using LIT = std::remove_pointer_t<decltype(tag)>;
+        AltoTensor<LIT>* AT = nullptr;
+        capture_stdout([&] { create_alto(X, &AT, nprtn); });
+        for (int p = 0; p < nprtn; ++p) {
+            prtn_id[p] = AT->prtn_id[p];
+            prtn_mask[p] = AT->prtn_mask[p];
+            for (int n = 0; n < nmode; ++n) prtn_mode_masks[(size_t)p * nmode + n] = AT->prtn_mode_masks[p * nmode + n];
+        }
+        destroy_alto(AT);
+    };
+    if (lit_bits == 128) run((unsigned __int128*)nullptr);
+    else run((unsigned long long*)nullptr);
+    DestroySparseTensor(X);
+    return 0;
+#else
+    (void)nmode; (void)dims; (void)nnz; (void)cidx; (void)vals; (void)nprtn; (void)lit_bits;
+    (void)prtn_id; (void)prtn_mask; (void)prtn_mode_masks;
+    return -1;
+#endif
 }
 
 } // extern "C"

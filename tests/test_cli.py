@@ -75,3 +75,24 @@ def test_cli_check_and_bench_modes(tmp_path):
     assert r.stderr.count("Results of mttkrp_alto is correct") == 3
     r = _run(["-l", "als", "-i", path, "--rank", 8, "-p", "-m", 3, "-t", 1])
     assert r.returncode == 0 and "ALTO runtime:" in r.stdout
+
+
+@pytest.mark.gpu
+@needs_cli
+def test_cli_generates_the_reference_poisson_tensor():
+    """cpd64 -d dims -s sparsity -r rank (MakeSparseTensor, main.cpp:652-675)
+    draws the tensor the reference's generator draws with the same OpenMP
+    thread count (the nonzero count it prints; the full tensor is compared
+    in test_poisson_gpu.py)."""
+    orc = pytest.importorskip("oracle.orc")
+    if not os.path.exists(orc.REF_SO_POISSON):
+        pytest.skip("reference generator library not built")
+    dims, sparsity, rank = (40, 30, 20), 0.5, 4
+    edges = int(sparsity * 40 * 30 * 20)
+    _, rv, _, _ = orc.RefPoisson().run(dims, edges, rank, 2)
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    r = subprocess.run([CLI, "-d", "40,30,20", "-s", str(sparsity), "-r", str(rank), "-l", "als", "-m", "2",
+                        "-x", "3"], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr
+    m = re.search(r"Creating a new tensor: [0-9.e+-]+ s \((\d+) nonzeros\)", r.stdout)
+    assert m and int(m.group(1)) == rv.shape[0], r.stdout
