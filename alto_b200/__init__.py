@@ -47,7 +47,7 @@ class _Info(C.Structure):
         ("dims", C.c_uint64 * MAX_MODES), ("mode_masks", (C.c_uint64 * 2) * MAX_MODES),
         ("cr_masks", (C.c_uint64 * 2) * MAX_MODES), ("alto_mask", C.c_uint64 * 2),
         ("alto_cr_mask", C.c_uint64 * 2), ("device_bytes", C.c_uint64), ("key_bytes", C.c_uint64),
-        ("nruns", C.c_int), ("plan_modes", C.c_int), ("plan_bytes", C.c_uint64),
+        ("nruns", C.c_int), ("plan_modes", C.c_int), ("plan_bytes", C.c_uint64), ("tma_err", C.c_int),
     ]
 
 
@@ -266,6 +266,7 @@ class AltoTensor:
             cr_masks=np.array([[inf.cr_masks[i][0], inf.cr_masks[i][1]] for i in range(nm)], np.uint64),
             alto_mask=(inf.alto_mask[0], inf.alto_mask[1]), device_bytes=inf.device_bytes,
             key_bytes=inf.key_bytes, nruns=inf.nruns, plan_modes=inf.plan_modes, plan_bytes=inf.plan_bytes,
+            tma_err=inf.tma_err,
         )
 
     def dump_alt_pext(self, stream=None):

@@ -1161,6 +1161,11 @@ altob_status altob_destroy(altob_tensor* t)
     for (int n = 0; n < ALTOB_MAX_MODES; ++n) dfree(t->d_plan[n]);
     dfree(t->scratch);
     dfree(t->hotbuf);
+    dfree(t->d_tma_err);
+    if (t->h_tma_err) {
+        cudaStreamSynchronize(0);  // the flag's last copy was ordered before the frees above
+        cudaFreeHost(t->h_tma_err);
+    }
     delete t;
     return ALTOB_OK;
 }
@@ -1190,6 +1195,7 @@ altob_status altob_get_info(const altob_tensor* t, altob_info* o)
     o->device_bytes = t->device_bytes;
     o->key_bytes = t->d_khi ? 16 : 8;
     o->nruns = t->nrun;
+    o->tma_err = t->h_tma_err ? (int)*t->h_tma_err : 0;
     for (int n = 0; n < t->nmode; ++n)
         if (t->d_plan[n]) {
             o->plan_modes |= 1 << n;

@@ -213,6 +213,10 @@ struct altob_tensor {
     size_t hotbuf_bytes = 0;
     // tile plans of the planned MTTKRP kernel, one per mode (built on first use)
     uint16_t* d_plan[ALTOB_MAX_MODES] = {nullptr};
+    // the TMA-staged kernel's wait-limit flag: on the device, and a pinned
+    // host copy refreshed after each of its launches
+    unsigned* d_tma_err = nullptr;
+    unsigned* h_tma_err = nullptr;
     // the stream of the last call that used the cached buffers or plans, and
     // an event recorded there: a call on another stream waits for it first
     cudaEvent_t use_ev = nullptr;

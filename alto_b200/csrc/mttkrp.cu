@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <type_traits>
 
 #include "mttkrp_launch.cuh"
 #include "mttkrp_plan.h"
@@ -113,6 +115,101 @@ const uint16_t* tensor_plan(altob_tensor* t, int mode, cudaStream_t st)
     return ensure_plan(t, mode, st) ? t->d_plan[mode] : nullptr;
 }
 
+// ---------------------------------------------- TMA-staged planned MTTKRP
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// Row-gather map of an I x R FP32 factor matrix (box: one row of R values).
+static bool row_map(CUtensorMap* m, const float* U, u64 rows, int R)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t dim[2] = {(cuuint64_t)R, (cuuint64_t)rows};
+    const cuuint64_t stride[1] = {(cuuint64_t)R * 4};
+    const cuuint32_t box[2] = {(cuuint32_t)R, 1};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)U, dim, stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int LPN, int S>
+static altob_status launch_tma_one(altob_tensor* t, TmaArgs& ta, const CUtensorMap& m0, const CUtensorMap& m1,
+                                   cudaStream_t st)
+{
+    using Sh = TmaShape<LPN, S>;
+    static std::atomic<size_t> configured{0};
+    const size_t smem = Sh::smem(ta.a.hot);
+    if (smem > configured.load()) {
+        ALTOB_CUDA(cudaFuncSetAttribute(k_planned_tma<LPN, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured.store(smem);
+    }
+    int bps = 0;
+    ALTOB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_planned_tma<LPN, S>, TMA_THREADS, smem));
+    if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "TMA MTTKRP kernel does not fit on an SM");
+    const unsigned grid = (unsigned)std::max<u64>(1, std::min<u64>(ta.a.ntiles, (u64)bps * num_sms()));
+    ALTOB_TRY(set_hot_acc(t, ta.a, grid, st));
+    k_planned_tma<LPN, S><<<grid, TMA_THREADS, smem, st>>>(ta, m0, m1);
+    ALTOB_LAUNCH_CHECK();
+    return ALTOB_OK;
+}
+
+// FP32, order 3, R = 4 * LPN with LPN in {4, 8, 16}, a tile plan, 16-byte
+// aligned factors: the TMA-staged kernel (ALTOB_TMA=1 selects it; 2 or 4
+// stages with ALTOB_TMA_STAGES).  Returns false when the case does not
+// qualify (the caller then runs the planned kernel).
+static bool tma_eligible(const altob_tensor* t, u64 R, bool planned)
+{
+    return planned && t->nmode == 3 && (R == 16 || R == 32 || R == 64) && env_int("ALTOB_TMA", 0) != 0 &&
+           encode_tiled() != nullptr;
+}
+
+static altob_status run_tma(altob_tensor* t, TiledArgs<float>& a, u64 R, cudaStream_t st)
+{
+    if (!t->d_tma_err) {
+        ALTOB_TRY(dmalloc_t(&t->d_tma_err, 4));
+        ALTOB_CUDA(cudaMemsetAsync(t->d_tma_err, 0, 4, st));
+        ALTOB_CUDA(cudaMallocHost((void**)&t->h_tma_err, 4));
+        *t->h_tma_err = 0;
+    }
+    if (*t->h_tma_err) return fail(ALTOB_ERR_CUDA, "an earlier TMA-staged MTTKRP ran out of a wait limit");
+    CUtensorMap m[2];
+    int k = 0;
+    for (int m_ = 0; m_ < 3; ++m_) {
+        if (m_ == a.target) continue;
+        if (!row_map(&m[k], a.U[m_], t->dims[m_], (int)R)) return fail(ALTOB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        ++k;
+    }
+    TmaArgs ta;
+    ta.a = a;
+    ta.err = t->d_tma_err;
+    const int stages = env_int("ALTOB_TMA_STAGES", 4) == 2 ? 2 : 4;
+    altob_status s;
+    if (R == 16) s = stages == 2 ? launch_tma_one<4, 2>(t, ta, m[0], m[1], st) : launch_tma_one<4, 4>(t, ta, m[0], m[1], st);
+    else if (R == 32) s = stages == 2 ? launch_tma_one<8, 2>(t, ta, m[0], m[1], st) : launch_tma_one<8, 4>(t, ta, m[0], m[1], st);
+    else s = stages == 2 ? launch_tma_one<16, 2>(t, ta, m[0], m[1], st) : launch_tma_one<16, 4>(t, ta, m[0], m[1], st);
+    ALTOB_TRY(s);
+    ALTOB_CUDA(cudaMemcpyAsync(t->h_tma_err, t->d_tma_err, 4, cudaMemcpyDeviceToHost, st));
+    return ALTOB_OK;
+}
+
 template <typename FT, typename VT>
 static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, void* dout, u64 R, bool phi,
                                  double eps, const u32* perm, bool cache, cudaStream_t st)
@@ -156,6 +253,9 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
         a.tile = PT_TILE;
         a.ntiles = (t->nnz + PT_TILE - 1) / PT_TILE;
         a.hslots = 0;
+        if constexpr (sizeof(FT) == 4 && std::is_same<VT, float>::value) {
+            if (tma_eligible(t, R, true)) return run_tma(t, a, R, st);
+        }
         c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn, PT_TILE, 2);
         ALTOB_TRY((launch_planned<FT, VT>(a, c, st, &bps)));
         if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned MTTKRP kernel does not fit on an SM");

@@ -5,7 +5,7 @@
 
 #include <atomic>
 
-#include "mttkrp_planned.cuh"
+#include "mttkrp_tma.cuh"
 
 namespace altob {
 

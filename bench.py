@@ -362,6 +362,8 @@ def run_altob(args):
     ms = t0.elapsed_time(t1)
     clocks = clk.stop()
     at_plan_modes = at.info()["plan_modes"]
+    free_b, total_b = torch.cuda.mem_get_info(dev)
+    dev_used_gb = (total_b - free_b) / 1e9  # the whole process's device memory after the timed steps
     ms = max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
     value = ws * nnz * 3 / (ms_step / 1e3) / 1e9
@@ -377,15 +379,16 @@ def run_altob(args):
     avg_ms = [statistics.mean(x) for x in launch_ms]
     achieved = sum(bytes_per_mode) / (sum(avg_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = None
+    traffic = l2 = None
     tf = os.path.join(ROOT, "profiles", "mttkrp_traffic.json")
     if os.path.exists(tf):
         try:
             with open(tf) as f:
                 tj = json.load(f)
             traffic = tj.get("per_launch_bytes_full_size")
+            l2 = tj.get("l2")
         except (OSError, ValueError):
-            traffic = None
+            traffic = l2 = None
 
     e2e = None
     if not args.no_e2e:
@@ -481,8 +484,11 @@ def run_altob(args):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                              "kernel": "k_planned (MTTKRP, tile plans)" if at_plan_modes == 7 else "k_grouped (MTTKRP)", "launch_ms_per_mode": avg_ms,
-                             "algorithmic_bytes_per_launch": bytes_per_mode},
+                             "algorithmic_bytes_per_launch": bytes_per_mode,
+                             "traffic_source": "profiles/mttkrp_traffic.json (two small captures, extrapolated)",
+                             "l2": l2},
                 "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu,
+                "device_mem_used_gb": dev_used_gb,
                 "fp64": f64, "batch": batch, "serve": serve}
         print(json.dumps(line), flush=True)
     return 0

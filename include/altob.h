@@ -80,6 +80,8 @@ typedef struct {
     int nruns;             /* high index words kept as a run table (0: none) */
     int plan_modes;        /* bit n set: mode n has a tile plan (MTTKRP) */
     uint64_t plan_bytes;   /* HBM held by the tile plans (2 B per nonzero and mode) */
+    int tma_err;           /* 1: a TMA-staged MTTKRP ran out of a wait limit (read after the
+                              stream of that call has been synchronised) */
 } altob_info;
 
 /* COO tensor in host memory (SparseTensor, sptensor.hpp:8-25): cidx is

@@ -138,3 +138,44 @@ def test_one_handle_two_streams():
     two = run([s1, s2])
     for a, b in zip(one, two):
         assert rel_fro(b, a) < 1e-6
+
+
+TMA_CASES = [
+    # dims, nnz, rank: tail tile, ranks 16/32/64, 65-bit keys (run table), skew (hot rows)
+    ((1000, 800, 600), 300_001, 32, "uniform"),
+    ((1000, 800, 600), 1500, 16, "uniform"),
+    ((200, 300, 400), 60_000, 64, "uniform"),
+    ((1 << 22, 1 << 21, 1 << 22), 2_000_000, 32, "zipf"),
+]
+
+
+@pytest.mark.parametrize("stages", ["2", "4"])
+@pytest.mark.parametrize("case", TMA_CASES)
+def test_tma_staged_kernel_matches_planned_and_fp64(case, stages, monkeypatch):
+    """The TMA-staged kernel (factor rows gathered into shared memory by
+    cp.async.bulk.tensor tile::gather4) against the planned kernel and the
+    FP64 result, FP32 within 1e-5; its wait-limit flag stays clear."""
+    torch = pytest.importorskip("torch")
+    dims, nnz, rank, kind = case
+    if kind == "zipf":
+        d, cidx, vals = synth.zipf_tensor(dims, nnz, 7, s=1.1)
+    else:
+        d, cidx, vals = synth.uniform_distinct(dims, nnz, seed=rank)
+    at32 = ab.create_alto(ab.SparseTensor.from_arrays(d, cidx, vals), 16, 0, val_dtype="f32")
+    at64 = ab.create_alto(ab.SparseTensor.from_arrays(d, cidx, vals), 16, 0)
+    for mode in range(3):
+        U = synth.random_factors(d, rank, seed=mode)
+        d64 = [torch.from_numpy(u).cuda() for u in U]
+        ab.mttkrp_alto_par(mode, d64, rank, at64, accumulate=False)
+        want = d64[mode].cpu().numpy()
+        got = {}
+        for tma in ("0", "1"):
+            monkeypatch.setenv("ALTOB_TMA", tma)
+            monkeypatch.setenv("ALTOB_TMA_STAGES", stages)
+            d32 = [torch.from_numpy(u).float().cuda() for u in U]
+            ab.mttkrp_alto_par(mode, d32, rank, at32, accumulate=False)
+            torch.cuda.synchronize()
+            got[tma] = d32[mode].double().cpu().numpy()
+        assert at32.info()["tma_err"] == 0
+        assert rel_fro(got["1"], want) < TOL32, (case, mode)
+        assert rel_fro(got["1"], got["0"]) < TOL32, (case, mode)
