@@ -113,7 +113,7 @@ template <typename FT, typename VT, int NM, int LPN, int V>
 altob_status launch_planned_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaStream_t st, int* bps)
 {
     static std::atomic<size_t> configured{0};
-    constexpr int mb = planned_min_blocks<FT, NM, V>();
+    constexpr int mb = planned_min_blocks<FT, NM, LPN>();
     if constexpr (mb > 0)
         return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, mb>, configured, &a, c, st, bps);
     else
@@ -152,7 +152,7 @@ altob_status launch_planned_batch_one(const BatchTiles<FT>& bt, const TiledCfg& 
 {
     static std::atomic<size_t> configured{0};
     constexpr int V = 16 / sizeof(FT);
-    constexpr int mb = planned_min_blocks<FT, NM, V>();
+    constexpr int mb = planned_min_blocks<FT, NM, LPN>();
     if constexpr (mb > 0)
         return launch_kernel(k_planned_batch_mb<FT, VT, NM, LPN, V, mb>, configured, &bt, c, st, bps);
     else

@@ -103,13 +103,27 @@ __global__ void __launch_bounds__(TILE / 2) k_tile_plan(KeySrc key, Fields fld, 
 // --------------------------------------------------------- planned MTTKRP
 
 // Resident blocks per SM each instance is compiled for (register cap), FP32:
-// 4 blocks of 8 warps for order 3 (as the grouped kernel) and 3 for orders
-// 4-5 (80-86 registers uncapped would allow only 2).
-template <typename FT, int NM, int VEC>
+// 5 blocks of 8 warps for order 3 (48 registers; the run loop waits on its
+// row gathers, so more resident warps hide more of that latency: 2.31 ms per
+// mode at 4 blocks, 2.17 ms at 5 on the 100.85M-nonzero Zipf tensor; 3
+// blocks: 2.53 ms) and 3 for orders 4-5 (80-86 registers uncapped would
+// allow only 2).  Ranks above 64 (32 lanes per nonzero) keep 4 blocks: at 48
+// registers their run loop spills.
+template <typename FT, int NM, int LPN>
 constexpr int planned_min_blocks()
 {
     if (sizeof(FT) != 4) return 0;
-    return NM == 3 ? 4 : 3;
+    return NM == 3 ? (LPN <= 16 ? 5 : 4) : 3;
+}
+
+// Nonzeros whose key, value and plan entry a thread loads together in the
+// scatter phase.  Four in flight were the register peak of the kernel; the
+// order-3 FP32 instance keeps one, which is what lets it fit 48 registers
+// without spilling in the run loop.
+template <typename FT, int NM>
+constexpr int planned_scatter_q()
+{
+    return (sizeof(FT) == 4 && NM == 3) ? 1 : 4;
 }
 
 // Records a lane group takes per tile (lpn lanes per nonzero).
@@ -128,13 +142,13 @@ inline size_t planned_smem(int nmode, size_t fsz, int hot, int lpn, int pt, int 
 // of its nonzeros (four in flight at a time), decodes the mode indices and
 // writes the record [target, other modes..., value] to its run-ordered slot
 // (one padding record per 2^PSH).
-template <typename FT, typename VT, int MM, int PT, int PSH>
+template <typename FT, typename VT, int MM, int PT, int PSH, int QM = 4>
 __device__ __forceinline__ void planned_scatter(const TiledArgs<FT>& a, u64 g0, int nvalid, u32* srec)
 {
     constexpr int RW = RecWords<FT, MM>::n;
     constexpr int FW = (int)(sizeof(FT) / 4);
     constexpr int IPT = PT / MT_THREADS;
-    constexpr int IPQ = IPT < 4 ? IPT : 4;
+    constexpr int IPQ = IPT < QM ? IPT : QM;
     const int tid = threadIdx.x, target = a.target;
     const VT* vals = reinterpret_cast<const VT*>(a.vals);
     TileHi th;
@@ -203,7 +217,7 @@ __device__ __forceinline__ void planned_tile(const TiledArgs<FT>& a, u64 ti, con
     const unsigned gmask = (0xffffffffu >> (32 - LPN)) << (q * LPN);
     const u64 g0 = ti * (u64)PT_TILE;
     const int nvalid = (int)min((u64)PT_TILE, a.nnz - g0);
-    planned_scatter<FT, VT, NM, PT_TILE, 5>(a, g0, nvalid, gs.srec);
+    planned_scatter<FT, VT, NM, PT_TILE, 5, planned_scatter_q<FT, NM>()>(a, g0, nvalid, gs.srec);
     __syncthreads();
     const int p0 = (warp * NPW + q) * IPG;
     const FT* Uo[NM - 1];
@@ -253,10 +267,8 @@ __device__ __forceinline__ void planned_body(const TiledArgs<FT>& a)
         u32* srec = b ? buf1 : buf0;
         const u64 g0 = ti * (u64)PT;
         const int nvalid = (int)min((u64)PT, a.nnz - g0);
-        TileHi th;
-        th.init(a.key, g0, PT);
         // ---- A: load key, value and plan entry; record into its sorted slot
-        planned_scatter<FT, VT, MM, PT, PSH>(a, g0, nvalid, srec);
+        planned_scatter<FT, VT, MM, PT, PSH, planned_scatter_q<FT, NM>()>(a, g0, nvalid, srec);
         // with two buffers one barrier per tile: the buffer written next tile
         // was last read before this barrier
         __syncthreads();
