@@ -400,6 +400,7 @@ struct BatchImpl : BatchBase {
     std::vector<std::unique_ptr<ClassRun<FT>>> classes;
     std::vector<std::unique_ptr<LaunchGroup<FT>>> groups;
     cudaStream_t cap_stream = nullptr;  // graph capture (never the legacy stream)
+    int prio = 0;                       // priority of the internal streams
     static constexpr int NFORK = 4;     // streams the launch groups of a mode spread over
     cudaStream_t fork_st[NFORK] = {nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[NFORK] = {nullptr};
@@ -814,7 +815,7 @@ struct BatchImpl : BatchBase {
     altob_status capture(double eps, int max_iters)
     {
         drop_graph();
-        if (!cap_stream) ALTOB_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        if (!cap_stream) ALTOB_CUDA(cudaStreamCreateWithPriority(&cap_stream, cudaStreamNonBlocking, prio));
         cudaGraph_t g = nullptr;
         ALTOB_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
         altob_status s = iteration(NORM_MAX, eps, max_iters, cap_stream);
@@ -1164,8 +1165,15 @@ struct BatchImpl : BatchBase {
             }
         }
         ALTOB_TRY(rebuild_groups(st));
+        // the internal streams take the priority of the caller's stream (a
+        // server runs short batched solves at a higher priority than long
+        // CP-APR requests)
+        if (cudaStreamGetPriority(st, &prio) != cudaSuccess) {
+            cudaGetLastError();
+            prio = 0;
+        }
         for (int i = 0; i < NFORK; ++i) {
-            ALTOB_CUDA(cudaStreamCreateWithFlags(&fork_st[i], cudaStreamNonBlocking));
+            ALTOB_CUDA(cudaStreamCreateWithPriority(&fork_st[i], cudaStreamNonBlocking, prio));
             ALTOB_CUDA(cudaEventCreateWithFlags(&join_ev[i], cudaEventDisableTiming));
         }
         ALTOB_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));

@@ -163,8 +163,15 @@ struct altob_server {
     void worker_main(int worker)
     {
         cudaSetDevice(device);
-        cudaStream_t st = nullptr;
-        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        // batched CP-ALS solves (short, many small launches) run at the
+        // device's highest stream priority, CP-APR requests (long streaming
+        // passes) at the lowest, so a batch admitted while long requests
+        // occupy the device still gets SMs as soon as blocks retire
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        cudaStream_t st = nullptr, st_hi = nullptr;
+        cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, lo);
+        cudaStreamCreateWithPriority(&st_hi, cudaStreamNonBlocking, cfg.plain ? lo : hi);
         for (;;) {
             std::vector<Job*> g;
             {
@@ -180,7 +187,7 @@ struct altob_server {
             }
             const double ts = now();
             for (Job* j : g) j->res.t_start = ts;
-            run(g, st);
+            run(g, g[0]->req.kind == ALTOB_REQ_CP_APR ? st : st_hi);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 const double te = now();
@@ -196,6 +203,7 @@ struct altob_server {
             cv_done.notify_all();
         }
         if (st) cudaStreamDestroy(st);
+        if (st_hi) cudaStreamDestroy(st_hi);
     }
 
     struct Model {

@@ -304,6 +304,14 @@ def run_altob(args):
     import alto_b200 as ab
 
     ws, rank, local = dist_setup()
+    # the batched and served objects first, each in a child process with the
+    # GPU to itself (no context of this process on the device yet)
+    batch = serve = None
+    if rank == 0 and ws == 1 and args.draws == DRAWS:
+        if not args.no_batch:
+            batch = sub_workload(args, "batch")
+        if not args.no_serve:
+            serve = sub_workload(args, "serve")
     torch.cuda.set_device(local)
     dist = None
     if ws > 1:
@@ -461,13 +469,6 @@ def run_altob(args):
         del out
     del at, U
     torch.cuda.empty_cache()
-
-    batch = serve = None
-    if rank == 0 and ws == 1 and args.draws == DRAWS:
-        if not args.no_batch:
-            batch = sub_workload(args, "batch")
-        if not args.no_serve:
-            serve = sub_workload(args, "serve")
 
     cpu = None
     if rank == 0 and not args.no_cpu and ws == 1:

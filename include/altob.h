@@ -343,7 +343,9 @@ ALTOB_API altob_status altob_batch_destroy(altob_batch* b);
  * is the queue head (policy 0) or the one with the least estimated work
  * (nonzeros x modes x iterations, x inner iterations for CP-APR, at an
  * assumed 10 Gnnz/s) after subtracting the time it has waited (policy 1:
- * short requests pass long ones, no request waits forever).  With plain = 1 every request runs
+ * short requests pass long ones, no request waits forever).  Batched CP-ALS
+ * solves run on a stream of the device's highest priority, CP-APR requests
+ * on one of the lowest.  With plain = 1 every request runs
  * alone through altob_cpd_als / altob_cp_apr (no batching).  Factors are
  * initialised on the device from the request's seed, identically alone or in
  * a batch.  The request's COO arrays (device, as for altob_create_device)
