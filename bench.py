@@ -387,7 +387,7 @@ def run_altob(args):
     avg_ms = [statistics.mean(x) for x in launch_ms]
     achieved = sum(bytes_per_mode) / (sum(avg_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = l2 = None
+    traffic = l2 = l1p = None
     tf = os.path.join(ROOT, "profiles", "mttkrp_traffic.json")
     if os.path.exists(tf):
         try:
@@ -395,8 +395,19 @@ def run_altob(args):
                 tj = json.load(f)
             traffic = tj.get("per_launch_bytes_full_size")
             l2 = tj.get("l2")
+            l1p = tj.get("l1_pipe")
         except (OSError, ValueError):
-            traffic = l2 = None
+            traffic = l2 = l1p = None
+    # the gather ceiling: the L1 data pipe retires one wavefront per SM cycle
+    # and the kernel needs wavefronts_per_nnz of them per nonzero (measured)
+    ceiling = None
+    if l1p and args.draws == DRAWS:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+        floor_ms = nnz * l1p["wavefronts_per_nnz"] / (sms * mhz * 1e6) * 1e3
+        ceiling = {"bound": "l1 data pipe (factor-row gathers)", "wavefronts_per_nnz": l1p["wavefronts_per_nnz"],
+                   "sms": sms, "sm_mhz": mhz, "floor_ms_per_launch": floor_ms,
+                   "frac": floor_ms / statistics.mean(avg_ms), "source": l1p["from"]}
 
     e2e = None
     if not args.no_e2e:
@@ -487,7 +498,7 @@ def run_altob(args):
                              "kernel": "k_planned (MTTKRP, tile plans)" if at_plan_modes == 7 else "k_grouped (MTTKRP)", "launch_ms_per_mode": avg_ms,
                              "algorithmic_bytes_per_launch": bytes_per_mode,
                              "traffic_source": "profiles/mttkrp_traffic.json (two small captures, extrapolated)",
-                             "l2": l2},
+                             "l2": l2, "ceiling": ceiling},
                 "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks, "cpu_baseline": cpu,
                 "device_mem_used_gb": dev_used_gb,
                 "fp64": f64, "batch": batch, "serve": serve}
@@ -558,6 +569,21 @@ def run_batch(args):
     ms = statistics.median(ms_all)
     value = args.batch_count / (ms / 1e3)
 
+    # cost of a replayed iteration in which every tensor has stopped (each
+    # kernel of the graph launches and finds no active tensor): solves of 2
+    # and 5 iterations with a tolerance every tensor meets after its second
+    # fit differ by three such replays (each length run twice: the second
+    # run replays the graph captured by the first)
+    idle = {}
+    for n_it in (2, 2, 5, 5):
+        reset32()
+        e0.record(stream)
+        b.solve(n_it, 1e300, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        idle[n_it] = e0.elapsed_time(e1)
+    idle_ms = (idle[5] - idle[2]) / 3
+
     base = None
     fit_err = None
     if not args.no_baseline:
@@ -594,6 +620,10 @@ def run_batch(args):
             "baseline_fp64_one_at_a_time": base,
             "speedup_vs_fp64_one_at_a_time": (value / base["value"]) if base else None,
             "fit_vs_fp64": fit_err, "autotune_s": tune_s, "schedule": desc,
+            "launches_per_iteration": launches_iter,
+            "idle_iteration_ms": idle_ms,
+            "idle_iteration_what": "a replayed iteration whose kernels all find their tensors stopped: "
+                                   "launch and scheduling cost of the graph, against ms_per_step / iterations",
             "gpu_launches": steps * (1 + iters * launches_iter), "clocks": clocks,
             "nnz_mode_rate_gnnz_s": sum(s[1] * len(s[0]) for s in shapes) * iters / (ms / 1e3) / 1e9}
     if rank == 0:
