@@ -256,7 +256,8 @@ static altob_status run_tiled_vt(altob_tensor* t, int mode, void* const* dU, voi
         if constexpr (sizeof(FT) == 4 && std::is_same<VT, float>::value) {
             if (tma_eligible(t, R, true)) return run_tma(t, a, R, st);
         }
-        c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn, PT_TILE, 2);
+        const int nbuf = t->nmode == 3 ? planned_nbuf<FT, 3>() : 2;
+        c.smem = planned_smem(t->nmode, sizeof(FT), a.hot, c.lpn, PT_TILE, nbuf);
         ALTOB_TRY((launch_planned<FT, VT>(a, c, st, &bps)));
         if (bps < 1) return fail(ALTOB_ERR_UNSUPPORTED, "planned MTTKRP kernel does not fit on an SM");
         c.grid = dim3((unsigned)std::max<u64>(1, std::min<u64>(a.ntiles, (u64)bps * num_sms())));

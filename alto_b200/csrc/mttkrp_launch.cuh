@@ -115,7 +115,8 @@ altob_status launch_planned_one(const TiledArgs<FT>& a, const TiledCfg& c, cudaS
     static std::atomic<size_t> configured{0};
     constexpr int mb = planned_min_blocks<FT, NM, LPN>();
     if constexpr (mb > 0)
-        return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, mb>, configured, &a, c, st, bps);
+        return launch_kernel(k_planned_mb<FT, VT, NM, LPN, V, mb, PT_TILE, planned_nbuf<FT, NM>()>, configured, &a, c, st,
+                             bps);
     else
         return launch_kernel(k_planned<FT, VT, NM, LPN, V>, configured, &a, c, st, bps);
 }

@@ -108,22 +108,34 @@ __global__ void __launch_bounds__(TILE / 2) k_tile_plan(KeySrc key, Fields fld, 
 // mode at 4 blocks, 2.17 ms at 5 on the 100.85M-nonzero Zipf tensor; 3
 // blocks: 2.53 ms) and 3 for orders 4-5 (80-86 registers uncapped would
 // allow only 2).  Ranks above 64 (32 lanes per nonzero) keep 4 blocks: at 48
-// registers their run loop spills.
+// registers their run loop spills.  FP64 order 3: 4 blocks (53-56
+// registers, one record buffer; 80 registers and 3 blocks uncapped: 23.1 ->
+// 21.9 ms per FP64 sweep of the same tensor; 5 blocks measured the same).
 template <typename FT, int NM, int LPN>
 constexpr int planned_min_blocks()
 {
-    if (sizeof(FT) != 4) return 0;
+    if (sizeof(FT) != 4) return NM == 3 ? 4 : 0;
     return NM == 3 ? (LPN <= 16 ? 5 : 4) : 3;
+}
+
+// Record buffers of the planned kernel: two (the next tile's scatter
+// overlaps this tile's runs) unless the records are 32 bytes and the kernel
+// targets 4 blocks per SM (order-3 FP64: two 33 KB buffers would leave room
+// for 3).
+template <typename FT, int NM>
+constexpr int planned_nbuf()
+{
+    return (sizeof(FT) == 8 && NM == 3) ? 1 : 2;
 }
 
 // Nonzeros whose key, value and plan entry a thread loads together in the
 // scatter phase.  Four in flight were the register peak of the kernel; the
-// order-3 FP32 instance keeps one, which is what lets it fit 48 registers
-// without spilling in the run loop.
+// order-3 instances keep one, which is what lets them fit their register
+// caps without spilling in the run loop.
 template <typename FT, int NM>
 constexpr int planned_scatter_q()
 {
-    return (sizeof(FT) == 4 && NM == 3) ? 1 : 4;
+    return NM == 3 ? 1 : 4;
 }
 
 // Records a lane group takes per tile (lpn lanes per nonzero).

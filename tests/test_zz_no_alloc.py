@@ -48,7 +48,12 @@ def test_loglik_noalloc_matches_loglik_on_two_calls(prec):
         torch.cuda.synchronize()
         stream = None if call == 0 else C.c_void_p(side.cuda_stream)
         want = _call(L.altob_loglik, at, ftype, UA, lA, rank, stream)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         got = _call(L.altob_loglik_noalloc, at, ftype, UB, lB, rank, stream)
+        torch.cuda.synchronize()
+        # nothing was allocated on the device by the call
+        assert torch.cuda.mem_get_info()[0] == free_before
         assert abs(got - want) <= tol * abs(want), (call, got, want)
         for a, b in zip(UA, UB):
             a, b = a.double().cpu().numpy(), b.double().cpu().numpy()
