@@ -229,6 +229,10 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
         }
     } pi_free{nullptr, nullptr, nullptr, nullptr};
     const u64 nnz = t->nnz;
+    // per-mode stride of the row-ordered stream: a multiple of 4 elements, so
+    // every mode's arrays start 16-byte aligned and may be read to a multiple
+    // of 4 past their end (bulk copies of whole 16-byte units)
+    const u64 nnzp = (nnz + 3) & ~3ull;
     AprPhi kind = nnz ? apr_phi_kind(t, R, sizeof(FT), max_inner) : PHI_OTF;
     // Memory can go to other streams between the choice and the allocations
     // (concurrent requests of a server): an allocation that fails falls back
@@ -242,15 +246,15 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
         pi_free.r = pi_free.i = pi_free.v = nullptr;
     };
     if (kind == PHI_ROWS) {
-        altob_status a = dmalloc_t(&rows, (size_t)N * nnz);
+        altob_status a = dmalloc_t(&rows, (size_t)N * nnzp);
         pi_free.r = rows;
-        if (a == ALTOB_OK) a = dmalloc_t(&inv, (size_t)N * nnz);
+        if (a == ALTOB_OK) a = dmalloc_t(&inv, (size_t)N * nnzp);
         pi_free.i = inv;
-        if (a == ALTOB_OK) a = dmalloc_t(&svals, (size_t)N * nnz);
+        if (a == ALTOB_OK) a = dmalloc_t(&svals, (size_t)N * nnzp);
         pi_free.v = svals;
         for (int n = 0; n < N && a == ALTOB_OK; ++n)
-            a = mode_order_device(t, n, ft, rows + (size_t)n * nnz, svals + (size_t)n * nnz, inv + (size_t)n * nnz,
-                                  st);
+            a = mode_order_device(t, n, ft, rows + (size_t)n * nnzp, svals + (size_t)n * nnzp,
+                                  inv + (size_t)n * nnzp, st);
         if (a == ALTOB_ERR_NOMEM) {
             drop_stream();
             kind = PHI_PRE;
@@ -282,13 +286,13 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
             }
             ALTOB_TRY(mul_cols<FT>(B, t->dims[n], R, s.lam, st));  // RedistributeLambda
             ALTOB_TRY(vec_fill(s.lam, R, 1.0, st));
-            const u32* inv_n = rows ? inv + (size_t)n * nnz : nullptr;
+            const u32* inv_n = rows ? inv + (size_t)n * nnzp : nullptr;
             if (pi) ALTOB_TRY(pi_device(t, n, ft, (void* const*)U, (u64)R, pi, st, inv_n));
             for (int inner = 0; inner < max_inner; ++inner) {
                 ninner[iter]++;
                 if (rows)
-                    ALTOB_TRY(phi_rows_device(t, n, ft, pi, rows + (size_t)n * nnz, svals + (size_t)n * nnz, B,
-                                              (u64)R, eps_div_zero, Phi[n], st));
+                    ALTOB_TRY(phi_rows_device(t, n, ft, pi, rows + (size_t)n * nnzp, svals + (size_t)n * nnzp, B,
+                                              (u64)R, eps_div_zero, Phi[n], st, true));
                 else if (pi) ALTOB_TRY(phi_pre_device(t, n, ft, pi, B, (u64)R, eps_div_zero, Phi[n], st));
                 else ALTOB_TRY(phi_device(t, n, ft, (void* const*)U, (u64)R, eps_div_zero, Phi[n], st));
                 if (dobench) {
@@ -350,6 +354,8 @@ static altob_status cp_apr_impl(altob_tensor* t, FT** U, FT* lam_io, int R, int 
     ALTOB_CUDA(cudaMemcpyAsync(&fit, s.fit, sizeof(double), cudaMemcpyDeviceToHost, st));
     ALTOB_TRY(vec_to<FT>(lam_io, s.lam, R, st));
     ALTOB_CUDA(cudaStreamSynchronize(st));
+    if (t->h_tma_err && *t->h_tma_err)
+        return fail(ALTOB_ERR_CUDA, "a bulk-copy-staged Phi pass ran out of a wait limit");
     if (summary) {
         summary[0] = ll;
         summary[1] = fit;

@@ -12,6 +12,7 @@
 
 #include "mttkrp_launch.cuh"
 #include "mttkrp_plan.h"
+#include "phi_rows_tma.cuh"
 
 namespace altob {
 
@@ -686,8 +687,72 @@ static void launch_phi_rows(int lpn, int ch, int grid, const FT* pi, const u32* 
 #undef PRK
 }
 
-altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
-                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st)
+// The handle's error word of the kernels with bounded waits (allocated on
+// first use); fails when an earlier launch ran out of a wait limit.
+static altob_status wait_error_word(altob_tensor* t, cudaStream_t st, unsigned** out)
+{
+    if (!t->d_tma_err) {
+        ALTOB_TRY(dmalloc_t(&t->d_tma_err, 4));
+        ALTOB_CUDA(cudaMemsetAsync(t->d_tma_err, 0, 4, st));
+        ALTOB_CUDA(cudaMallocHost((void**)&t->h_tma_err, 4));
+        *t->h_tma_err = 0;
+    }
+    if (*t->h_tma_err) return fail(ALTOB_ERR_CUDA, "an earlier bulk-copy-staged kernel ran out of a wait limit");
+    *out = t->d_tma_err;
+    return ALTOB_OK;
+}
+
+// Row-ordered Phi with the stream staged by bulk copies (phi_rows_tma.cuh).
+template <typename FT, int VEC>
+static altob_status launch_phi_rows_tma(altob_tensor* t, int lpn, const FT* pi, const u32* rows, const FT* vals,
+                                        const FT* B, FT* phi, u64 nnz, int R, FT eps, cudaStream_t st)
+{
+    PhiTmaArgs<FT> a;
+    a.Pi = pi;
+    a.rows = rows;
+    a.vals = vals;
+    a.B = B;
+    a.Phi = phi;
+    a.nnz = nnz;
+    a.R = R;
+    a.eps = eps;
+    ALTOB_TRY(wait_error_word(t, st, &a.err));
+    const u64 vg = (u64)PX_CONSUMERS * (32 / lpn);
+    a.S = std::max<u64>(vg, (u64)PX_ROW_BYTES / ((u64)R * sizeof(FT)) / vg * vg);
+    a.nstage = (nnz + a.S - 1) / a.S;
+    const u64 grid0 = std::min<u64>(a.nstage, (u64)num_sms() * 2);
+    a.per_cta = (a.nstage + grid0 - 1) / grid0;
+    const unsigned grid = (unsigned)((a.nstage + a.per_cta - 1) / a.per_cta);
+    const size_t smem = phi_tma_smem(a.S, R, (int)sizeof(FT));
+    // the shared-memory limit is set once per kernel instance (one slot per
+    // lane count; every instance of an FT has the same function type)
+    static std::atomic<size_t> configured[6] = {};
+    auto go = [&](void (*kern)(const PhiTmaArgs<FT>), int slot) -> altob_status {
+        if (smem > configured[slot].load()) {
+            ALTOB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            configured[slot].store(smem);
+        }
+        kern<<<grid, PX_THREADS, smem, st>>>(a);
+        return ALTOB_OK;
+    };
+    altob_status s;
+    switch (lpn) {
+    case 1: s = go(k_phi_rows_tma<FT, VEC, 1>, 0); break;
+    case 2: s = go(k_phi_rows_tma<FT, VEC, 2>, 1); break;
+    case 4: s = go(k_phi_rows_tma<FT, VEC, 4>, 2); break;
+    case 8: s = go(k_phi_rows_tma<FT, VEC, 8>, 3); break;
+    case 16: s = go(k_phi_rows_tma<FT, VEC, 16>, 4); break;
+    default: s = go(k_phi_rows_tma<FT, VEC, 32>, 5); break;
+    }
+    ALTOB_TRY(s);
+    ALTOB_LAUNCH_CHECK();
+    ALTOB_CUDA(cudaMemcpyAsync(t->h_tma_err, t->d_tma_err, 4, cudaMemcpyDeviceToHost, st));
+    return ALTOB_OK;
+}
+
+altob_status phi_rows_device(altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
+                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st,
+                             bool pad4)
 {
     if (!t || !dpi || !rows || !svals || !dB || !dphi) return fail(ALTOB_ERR_ARG, "NULL argument");
     if (mode < 0 || mode >= t->nmode) return fail(ALTOB_ERR_ARG, "mode out of range");
@@ -705,6 +770,15 @@ altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, co
     const int per_sm = ch * ve * (int)fsz <= 16 ? (fsz == 4 ? 4 : 3) : 2;  // pr_min_blocks: one wave
     const int grid = (int)std::max<u64>(1, std::min<u64>((nchunks + 7) / 8, (u64)num_sms() * per_sm));
     const u64 nnz = t->nnz;
+    // the stream staged by bulk copies: one vector chunk per lane, whole
+    // 16-byte rows, stream arrays readable to a multiple of 4 past the end
+    if (pad4 && vec && ch == 1 && (R * fsz) % 16 == 0 && env_int("ALTOB_PHI_TMA", 1)) {
+        if (ft == ALTOB_F64)
+            return launch_phi_rows_tma<double, 2>(t, lpn, (const double*)dpi, rows, (const double*)svals,
+                                                  (const double*)dB, (double*)dphi, nnz, (int)R, eps, st);
+        return launch_phi_rows_tma<float, 4>(t, lpn, (const float*)dpi, rows, (const float*)svals, (const float*)dB,
+                                             (float*)dphi, nnz, (int)R, (float)eps, st);
+    }
     if (ft == ALTOB_F64) {
         if (vec) launch_phi_rows<double, 2>(lpn, ch, grid, (const double*)dpi, rows, (const double*)svals,
                                             (const double*)dB, (double*)dphi, nnz, (int)R, eps, st);

@@ -33,7 +33,11 @@ altob_status phi_pre_device(altob_tensor* t, int mode, altob_dtype ft, const voi
 // nonzero i; and Phi computed from it and the stream-ordered Khatri-Rao rows.
 altob_status mode_order_device(altob_tensor* t, int mode, altob_dtype ft, u32* rows, void* svals, u32* inv,
                                cudaStream_t st);
-altob_status phi_rows_device(const altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
-                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st);
+// pad4: rows and svals may be read up to a multiple of 4 elements past the
+// mode's nnz (and start 16-byte aligned), which lets the stream be staged by
+// bulk copies.
+altob_status phi_rows_device(altob_tensor* t, int mode, altob_dtype ft, const void* dpi, const u32* rows,
+                             const void* svals, const void* dB, u64 R, double eps, void* dphi, cudaStream_t st,
+                             bool pad4 = false);
 
 }  // namespace altob
