@@ -770,9 +770,10 @@ altob_status phi_rows_device(altob_tensor* t, int mode, altob_dtype ft, const vo
     const int per_sm = ch * ve * (int)fsz <= 16 ? (fsz == 4 ? 4 : 3) : 2;  // pr_min_blocks: one wave
     const int grid = (int)std::max<u64>(1, std::min<u64>((nchunks + 7) / 8, (u64)num_sms() * per_sm));
     const u64 nnz = t->nnz;
-    // the stream staged by bulk copies: one vector chunk per lane, whole
+    // the stream staged by bulk copies (ALTOB_PHI_TMA=1; measured no faster
+    // than the register-staged kernel): one vector chunk per lane, whole
     // 16-byte rows, stream arrays readable to a multiple of 4 past the end
-    if (pad4 && vec && ch == 1 && (R * fsz) % 16 == 0 && env_int("ALTOB_PHI_TMA", 1)) {
+    if (pad4 && vec && ch == 1 && (R * fsz) % 16 == 0 && env_int("ALTOB_PHI_TMA", 0)) {
         if (ft == ALTOB_F64)
             return launch_phi_rows_tma<double, 2>(t, lpn, (const double*)dpi, rows, (const double*)svals,
                                                   (const double*)dB, (double*)dphi, nnz, (int)R, eps, st);

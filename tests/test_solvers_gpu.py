@@ -138,6 +138,27 @@ def test_gpu_cp_apr_row_stream_matches_on_the_fly(rank, monkeypatch):
             assert rel_fro(Ma.U[n], Mb.U[n]) < (1e-9 if dtype == np.float64 else 1e-3), n
 
 
+@pytest.mark.parametrize("rank", [4, 16, 24, 64])
+def test_gpu_cp_apr_bulk_copy_phi_matches_register_staged(rank, monkeypatch):
+    """The row-ordered Phi staged in shared memory by bulk copies
+    (ALTOB_PHI_TMA=1) against the register-staged one, FP64 and FP32, fixed
+    inner counts; a nonzero count that is not a multiple of 4 exercises the
+    padded tail of the stream arrays."""
+    dims, cidx, vals = synth.poisson_kruskal((300, 120, 80, 15), 5, 150_003, seed=22)
+    at = ab.create_alto(_coo(dims, cidx, vals), 8, 0, val_dtype="u32")
+    monkeypatch.setenv("ALTOB_APR_PHI", "rows")
+    for dtype, tol in ((np.float64, 1e-10), (np.float32, 1e-4)):
+        res = {}
+        for tma in ("1", "0"):
+            monkeypatch.setenv("ALTOB_PHI_TMA", tma)
+            M = ab.random_init_factors(dims, rank, 3, dtype=dtype)
+            res[tma] = (ab.cp_apr_alto(at, M, 4, 5, epsilon=0.0, dobench=True), M)
+        (ra, Ma), (rb, Mb) = res["1"], res["0"]
+        assert abs(ra["loglik"] - rb["loglik"]) <= tol * abs(rb["loglik"])
+        for n in range(4):
+            assert rel_fro(Ma.U[n], Mb.U[n]) < (1e-9 if dtype == np.float64 else 1e-3), n
+
+
 def test_gpu_phi_and_loglik_match_oracle(oracle):
     torch = pytest.importorskip("torch")
     dims, cidx, vals = synth.poisson_kruskal((120, 90, 60), 5, 50_000, seed=8)
