@@ -716,6 +716,15 @@ static altob_status launch_phi_rows_tma(altob_tensor* t, int lpn, const FT* pi, 
     a.nnz = nnz;
     a.R = R;
     a.eps = eps;
+    a.wait_limit = TMA_WAIT_LIMIT;
+    a.stall = 0;
+    if (env_int("ALTOB_TEST_STALL_PHI", 0)) {
+        // failure test: the producer warp issues nothing, so the consumers'
+        // waits run out after a short limit (no copy is ever in flight) and
+        // the kernel reports it through the handle's error word
+        a.stall = 1;
+        a.wait_limit = 1u << 12;
+    }
     ALTOB_TRY(wait_error_word(t, st, &a.err));
     const u64 vg = (u64)PX_CONSUMERS * (32 / lpn);
     a.S = std::max<u64>(vg, (u64)PX_ROW_BYTES / ((u64)R * sizeof(FT)) / vg * vg);

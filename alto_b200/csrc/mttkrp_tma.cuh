@@ -63,9 +63,10 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar)
 // Waits (bounded) for the phase of the given parity; false when it ran out
 // or when another thread of the CTA has given up already (*abort set): after
 // the first wait that runs out, every later one returns at once.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int* abort)
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int* abort,
+                                          unsigned limit = TMA_WAIT_LIMIT)
 {
-    for (unsigned it = 0; it < TMA_WAIT_LIMIT; ++it) {
+    for (unsigned it = 0; it < limit; ++it) {
         unsigned done;
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"

@@ -54,6 +54,9 @@ struct PhiTmaArgs {
     int R;
     FT eps;
     unsigned* err;
+    unsigned wait_limit;  // polls per mbarrier wait
+    int stall;            // 1: the producer issues no copies (a failure test: every
+                          // consumer wait then runs out and the kernel reports it)
 };
 
 // Byte offsets of one stage: rows of the Khatri-Rao stream | target rows |
@@ -107,12 +110,12 @@ __global__ void __launch_bounds__(PX_THREADS, 2) k_phi_rows_tma(const PhiTmaArgs
     bool ok = true;
     u64 used = 0;  // stages of the ring used so far
     if (producer) {
-        if (lane == 0) {
+        if (lane == 0 && !a.stall) {
             for (u64 t = t0; t < t1; ++t, ++used) {
                 const int sl = (int)(used % PX_STAGES);
                 const unsigned par = (unsigned)((used / PX_STAGES) & 1);
-                ok = mbar_wait(empty0 + 8 * sl, par ^ 1u, abort) && ok;
-                if (!ok) break;  // a consumer gave up: issue nothing more
+                ok = mbar_wait(empty0 + 8 * sl, par ^ 1u, abort, a.wait_limit) && ok;
+                if (!ok || *abort) break;  // a wait gave up: issue nothing more
                 const u64 p0 = t * a.S;
                 const u64 n = min(a.S, a.nnz - p0);
                 const u64 n4 = (n + 3) & ~3ull;  // the stream arrays are readable to a multiple of 4
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(PX_THREADS, 2) k_phi_rows_tma(const PhiTmaArgs
                 const u64 uses = used / PX_STAGES + ((u64)sl < used % PX_STAGES ? 1 : 0);
                 if (uses) {
                     volatile int keep_waiting = 0;
-                    mbar_wait(full0 + 8 * sl, (unsigned)((uses - 1) & 1), &keep_waiting);
+                    mbar_wait(full0 + 8 * sl, (unsigned)((uses - 1) & 1), &keep_waiting, a.wait_limit);
                 }
             }
         }
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(PX_THREADS, 2) k_phi_rows_tma(const PhiTmaArgs
         for (u64 t = t0; t < t1; ++t, ++used) {
             const int sl = (int)(used % PX_STAGES);
             const unsigned par = (unsigned)((used / PX_STAGES) & 1);
-            const bool arrived = __all_sync(0xffffffffu, mbar_wait(full0 + 8 * sl, par, abort));
+            const bool arrived = __all_sync(0xffffffffu, mbar_wait(full0 + 8 * sl, par, abort, a.wait_limit));
             ok = arrived && ok;
             if (arrived) {
                 const unsigned char* sb = smem + (size_t)sl * L.stage;

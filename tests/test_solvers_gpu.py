@@ -159,6 +159,32 @@ def test_gpu_cp_apr_bulk_copy_phi_matches_register_staged(rank, monkeypatch):
             assert rel_fro(Ma.U[n], Mb.U[n]) < (1e-9 if dtype == np.float64 else 1e-3), n
 
 
+def test_gpu_bulk_copy_phi_wait_runs_out_and_reports(monkeypatch):
+    """Failure detection without a GPU fault: the bulk-copy-staged Phi's
+    producer warp is told to issue nothing (ALTOB_TEST_STALL_PHI=1), so every
+    consumer wait on a stage's mbarrier runs out after a short limit; the
+    kernel returns normally, records the failure in the handle's error word,
+    and the solve reports ALTOB_ERR_CUDA.  The GPU stays usable: a fresh
+    handle then solves normally and equals the register-staged solve."""
+    dims, cidx, vals = synth.poisson_kruskal((300, 120, 80, 15), 5, 60_000, seed=23)
+    rank = 16
+    monkeypatch.setenv("ALTOB_APR_PHI", "rows")
+    monkeypatch.setenv("ALTOB_PHI_TMA", "1")
+    monkeypatch.setenv("ALTOB_TEST_STALL_PHI", "1")
+    at = ab.create_alto(_coo(dims, cidx, vals), 8, 0, val_dtype="u32")
+    M = ab.random_init_factors(dims, rank, 3, dtype=np.float32)
+    with pytest.raises(ab.AltobError, match="wait limit"):
+        ab.cp_apr_alto(at, M, 2, 3, epsilon=0.0, dobench=True)
+    monkeypatch.delenv("ALTOB_TEST_STALL_PHI")
+    res = {}
+    for tma in ("1", "0"):
+        monkeypatch.setenv("ALTOB_PHI_TMA", tma)
+        fresh = ab.create_alto(_coo(dims, cidx, vals), 8, 0, val_dtype="u32")
+        M = ab.random_init_factors(dims, rank, 3, dtype=np.float32)
+        res[tma] = ab.cp_apr_alto(fresh, M, 2, 3, epsilon=0.0, dobench=True)
+    assert abs(res["1"]["loglik"] - res["0"]["loglik"]) <= 1e-4 * abs(res["0"]["loglik"])
+
+
 def test_gpu_phi_and_loglik_match_oracle(oracle):
     torch = pytest.importorskip("torch")
     dims, cidx, vals = synth.poisson_kruskal((120, 90, 60), 5, 50_000, seed=8)
