@@ -13,7 +13,7 @@
 // waiting on those loads (long-scoreboard stalls at 0.71 of the copy
 // bandwidth).  Here a producer warp streams it into a ring of shared-memory
 // stages with cp.async.bulk (one-dimensional bulk copies, completion counted
-// on an mbarrier), several stages ahead of the eight consumer warps, so the
+// on an mbarrier), several stages ahead of the sixteen consumer warps, so the
 // bytes in flight no longer hold registers.  Each CTA takes a contiguous
 // range of stages; a lane group ("virtual group" vg of the CTA) takes the
 // stream positions congruent to vg modulo the CTA's group count, so it sees
@@ -28,7 +28,7 @@
 
 namespace altob {
 
-constexpr int PX_CONSUMERS = 8;                       // consumer warps
+constexpr int PX_CONSUMERS = 16;                      // consumer warps
 constexpr int PX_THREADS = (PX_CONSUMERS + 1) * 32;   // + one producer warp
 constexpr int PX_STAGES = 3;
 constexpr int PX_ROW_BYTES = 24 * 1024;               // Khatri-Rao rows per stage (at most)
