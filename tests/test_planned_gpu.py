@@ -23,6 +23,9 @@ CASES = [
     ((64, 64, 64, 64, 64), 50_000, 16),
     ((200, 300, 400), 50_000, 2),
     ((200, 300, 400), 50_000, 24),   # lanes past the rank
+    ((1000, 800, 600), 200_000, 64),  # order 3, 16 lanes per nonzero (5 blocks per SM in FP32)
+    ((1000, 800, 600), 100_000, 48),  # 16 lanes, four past the rank
+    ((500, 400, 300), 60_000, 100),   # 32 lanes (4 blocks per SM in FP32), seven past the rank
 ]
 
 
@@ -39,7 +42,8 @@ def _restore(old):
         os.environ["ALTOB_PLAN"] = old
 
 
-@pytest.mark.parametrize("case", CASES)
+# FP64 ranks above 64 need two vector chunks per lane: the grouped kernel
+@pytest.mark.parametrize("case", [c for c in CASES if c[2] <= 64])
 def test_planned_fp64_matches_oracle(oracle, case):
     torch = pytest.importorskip("torch")
     dims, nnz, rank = case
@@ -58,7 +62,7 @@ def test_planned_fp64_matches_oracle(oracle, case):
         assert at.info()["plan_modes"] >> mode & 1, "the tile plan was not used"
 
 
-@pytest.mark.parametrize("case", CASES[:4] + CASES[5:6])
+@pytest.mark.parametrize("case", CASES[:4] + CASES[5:6] + CASES[8:])
 def test_planned_fp32_matches_grouped_and_fp64(case):
     torch = pytest.importorskip("torch")
     dims, nnz, rank = case
