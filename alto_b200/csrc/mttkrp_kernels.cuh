@@ -161,6 +161,7 @@ struct TiledArgs {
     int hot;       // per-CTA hot-row slots (power of two; 0: none), grouped kernel only
     FT* hot_acc;   // gridDim.x x hot x R accumulators, one private region per CTA
     const uint16_t* plan;  // tile plan of the target mode (planned kernel only)
+    int hot_minrun;        // shortest run through the hot-row table (0: GT_HOT_MINRUN)
 };
 
 // Dynamic shared-memory bytes of k_tiled.
@@ -693,6 +694,7 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
     for (int k = 0; k < MM - 1; ++k) Ub[k] = Uo[k] + col;
     u32 cur = 0xffffffffu;
     int len = 0;
+    const int hmin = a.hot_minrun ? a.hot_minrun : GT_HOT_MINRUN;
     FT acc[1][VEC];
 #pragma unroll
     for (int e = 0; e < VEC; ++e) acc[0][e] = FT(0);
@@ -705,7 +707,7 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
         for (int k = 0; k < MM - 1; ++k) vmul<FT, VEC>(x[0], y[k]);
         if (w[0] != cur) {
             if (cur != 0xffffffffu)
-                flush_run<FT, VEC, 1, LPN>(a.out, gs, len >= GT_HOT_MINRUN ? a.hot : 0, a.hot_acc, gmask, cur, R,
+                flush_run<FT, VEC, 1, LPN>(a.out, gs, len >= hmin ? a.hot : 0, a.hot_acc, gmask, cur, R,
                                            sub, acc);
             cur = w[0];
             len = 1;
@@ -739,7 +741,7 @@ __device__ __forceinline__ void lean_runs(const TiledArgs<FT>& a, const GroupedS
         add(w0, y0);
     }
     if (cur != 0xffffffffu)
-        flush_run<FT, VEC, 1, LPN>(a.out, gs, len >= GT_HOT_MINRUN ? a.hot : 0, a.hot_acc, gmask, cur, R, sub, acc);
+        flush_run<FT, VEC, 1, LPN>(a.out, gs, len >= hmin ? a.hot : 0, a.hot_acc, gmask, cur, R, sub, acc);
 }
 
 // Shared-memory work areas of the grouped kernels (tags and counts must be
